@@ -1,0 +1,233 @@
+/*
+ * cudafoam.h -- C ABI of the B200 (sm_100a) Krylov hot path behind the
+ * cudaPCG / cudaPBiCGStab lduMatrix::solver plugins.
+ *
+ * The library is a drop-in for the device backend and the FP64 driver of
+ * the metal4Foam plugin (scotCW/metal4Foam).  Each entry point names the
+ * reference interface it replaces:
+ *
+ *   backend   src/metal4Foam/backend/metalFoamBackend.H:37-115
+ *   driver    src/metal4Foam/solvers/metalFoamSolver.H:60-108 (solveImpl)
+ *   plugins   src/metal4Foam/solvers/metalPCG.H:47-92,
+ *             src/metal4Foam/solvers/metalPBiCGStab.C:16-59
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Host pointers unless the name ends in
+ *    _device (then CUDA device pointers on the context's device).
+ *  - Every call returns an int status (CF_OK = 0).  No exception crosses the
+ *    ABI; cf_last_error() returns a message for the calling thread.
+ *  - Breakdown and stagnation are not errors: like the reference
+ *    (metalFoamBackend::Stats, metalFoamBackend.H:41-50) they are reported as
+ *    flags in the statistics structs.
+ *  - One context per (mesh, field), the reference's cache key
+ *    (metalFoamSolver.C:57-74).  A context is not shared between threads.
+ *  - The caller owns host arrays; the context owns its device buffers.
+ *  - Labels are int32 and scalars FP64 (the reference's static_asserts,
+ *    metalFoamSolver.C:18-27).
+ */
+#ifndef CUDAFOAM_H
+#define CUDAFOAM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CF_ABI_VERSION 1
+
+/* status codes */
+enum
+{
+    CF_OK = 0,
+    CF_ERR_INVALID_ARG = 1,     /* null pointer, negative size, bad option */
+    CF_ERR_BAD_ADDRESSING = 2,  /* faces not in LDU order / inconsistent   */
+    CF_ERR_NO_TOPOLOGY = 3,     /* cf_set_topology not called              */
+    CF_ERR_NO_COEFFS = 4,       /* cf_set_coeffs not called                */
+    CF_ERR_CUDA = 5,            /* a CUDA runtime call failed              */
+    CF_ERR_NO_DEVICE = 6,       /* no usable sm_100 device                 */
+    CF_ERR_DEVICE_TIMEOUT = 7,  /* a bounded device-side wait expired      */
+    CF_ERR_UNSUPPORTED = 8,     /* option combination not supported        */
+    CF_ERR_TOO_LARGE = 9        /* size beyond a stated maximum            */
+};
+
+/* solver selection (the plugin names cudaPCG / cudaPBiCGStab) */
+enum { CF_SOLVER_PCG = 0, CF_SOLVER_PBICGSTAB = 1 };
+
+/* deflate on|off|auto (metalFoamSolver.C:170-190) */
+enum { CF_DEFLATE_AUTO = 0, CF_DEFLATE_ON = 1, CF_DEFLATE_OFF = 2 };
+
+/* internal cell ordering chosen at cf_set_topology */
+enum { CF_REORDER_NONE = 0, CF_REORDER_RCM = 1, CF_REORDER_AUTO = 2 };
+
+typedef struct cf_context cf_context;
+
+/* metalFoamBackend::Stats (metalFoamBackend.H:41-50) */
+typedef struct
+{
+    int32_t nIterations;      /* inner FP32 iterations performed          */
+    int32_t converged;        /* hit the requested L1 target              */
+    int32_t singular;         /* breakdown (non-finite scalars)           */
+    int32_t stagnated;        /* 50 iterations without progress           */
+    double finalResSum;       /* inner L1 sum |r| at exit (unnormalised)  */
+    double tGpuSeconds;       /* device time of the inner loop            */
+    double tWallSeconds;      /* host wall time of the call               */
+} cf_inner_stats;
+
+/* fvSolution controls: tolerance, relTol, maxIter, minIter (read by
+ * OpenFOAM's lduMatrix::solver) and the plugin sub-dictionary keys
+ * (metalFoamSolver.C:170-171,224-227,259-263). */
+typedef struct
+{
+    double tolerance;          /* default 1e-6                             */
+    double relTol;             /* default 0                                */
+    int32_t maxIter;           /* default 1000                             */
+    int32_t minIter;           /* default 0                                */
+    int32_t maxRestarts;       /* default 8                                */
+    int32_t iterationsPerSync; /* default 1: convergence test granularity  */
+    int32_t deflate;           /* CF_DEFLATE_*, default AUTO (PCG only)    */
+    int32_t chebyshevOrder;    /* default 8 (PCG); BiCGStab always 1       */
+    double chebyshevRatio;     /* default 30                               */
+    int32_t profile;           /* print a timing line per solve           */
+    int32_t verbose;           /* print a residual line per restart        */
+    int32_t graph;             /* 1 (default): inner loop as a device-side
+                                  CUDA-graph while loop, no host sync per
+                                  iteration; 0: one host sync per batch of
+                                  iterationsPerSync, as the reference      */
+    int32_t reserved;
+} cf_options;
+
+/* solverPerformance plus the reference's profile/verbose figures
+ * (metalFoamSolver.C:127-128,363-365,417-426). */
+typedef struct
+{
+    double initialResidual;    /* FP64 sum|b - A psi0| / normFactor        */
+    double finalResidual;      /* FP64 sum|b - A psi|  / normFactor        */
+    int32_t nIterations;       /* total inner iterations                   */
+    int32_t nRestarts;         /* outer refinement passes - 1 (`outer`)    */
+    int32_t converged;
+    int32_t singular;
+    int32_t stagnated;         /* last inner solve stagnated               */
+    int32_t deflated;          /* constant-mode deflation chosen           */
+    int32_t polished;          /* hybrid polish switched to the exact diag */
+    int32_t solved;            /* 0: the entry test had already converged  */
+    double normFactor;
+    double chebBeta;           /* Gershgorin bound of D^-1 A               */
+    double finalResSum32;      /* last inner L1 sum (unnormalised)         */
+    double residualL2;         /* ||b - A psi||_2 / ||b||_2 at exit        */
+    double tConvert;           /* seconds: coefficient staging             */
+    double tInner;             /* seconds: host wall time of inner solves  */
+    double tGpu;               /* seconds: device time of inner solves     */
+    double tSolve;             /* seconds: device time of the whole solve  */
+} cf_performance;
+
+/* ------------------------------------------------------------ library */
+
+int cf_abi_version(void);
+/* message of the last failed call on this thread ("" if none) */
+const char* cf_last_error(void);
+/* fills defaults: tolerance 1e-6, relTol 0, maxIter 1000, minIter 0,
+ * maxRestarts 8, iterationsPerSync 1, deflate auto, chebyshevOrder 8,
+ * chebyshevRatio 30, graph 1 */
+void cf_options_default(cf_options* opts);
+
+/* ------------------------------------------------------------ context */
+
+/* metalFoamBackend::metalFoamBackend / Impl::init (metalFoamBackend.C:192-282,
+ * 422-430): binds a CUDA device (must be sm_100), creates a stream. */
+int cf_context_create(cf_context** out, int32_t device);
+int cf_context_destroy(cf_context* ctx);
+/* metalFoamBackend::good (metalFoamBackend.H:106) */
+int cf_context_good(const cf_context* ctx);
+/* metalFoamBackend::description (metalFoamBackend.H:109) */
+const char* cf_context_description(const cf_context* ctx);
+/* Use the caller's cudaStream_t (e.g. torch.cuda.current_stream()) for
+ * all later work of this context; NULL restores the context's own stream. */
+int cf_context_set_stream(cf_context* ctx, void* stream);
+/* Internal row ordering for the next cf_set_topology (default AUTO: RCM
+ * for meshes above 65536 cells).  Results are returned in the caller's
+ * ordering either way. */
+int cf_context_set_reorder(cf_context* ctx, int32_t mode);
+/* Number of kernels this context has launched so far (graph bodies are
+ * counted once per executed iteration).  Diagnostic; no reference
+ * counterpart. */
+int cf_context_kernel_launches(const cf_context* ctx, long long* count);
+
+/* ------------------------------------------------------------ matrix */
+
+/* metalFoamBackend::setTopology (metalFoamBackend.H:60-69,
+ * metalFoamBackend.C:454-519).  The five lduAddressing arrays; validated
+ * (ranges, LDU order, consistency of ownerStart/losort/losortStart) and
+ * cached on (nCells, nFaces, lowAddr, uppAddr) identity like the
+ * reference.  Builds the device layout once per mesh. */
+int cf_set_topology(cf_context* ctx, int32_t nCells, int32_t nFaces,
+                    const int32_t* lowAddr, const int32_t* uppAddr,
+                    const int32_t* ownStartAddr, const int32_t* losortAddr,
+                    const int32_t* losortStartAddr);
+
+/* metalFoamBackend::setCoeffs (metalFoamBackend.H:74-79,
+ * metalFoamBackend.C:522-565).  FP64 diag[nCells], upper[nFaces],
+ * lower[nFaces] (NULL: symmetric).  Keeps FP64 copies on the device and
+ * stages FP32 copies plus rD = float(1/diag) there.  *tConvert (may be
+ * NULL) receives the seconds spent, like the reference's return value. */
+int cf_set_coeffs(cf_context* ctx, const double* diag, const double* upper,
+                  const double* lower, double* tConvert);
+/* Same from device pointers (no host copy). */
+int cf_set_coeffs_device(cf_context* ctx, const double* diag,
+                         const double* upper, const double* lower);
+
+/* ------------------------------------------------------------ inner solves */
+
+/* metalFoamBackend::pcg (metalFoamBackend.H:83-92, .C:568-732): FP32 PCG on
+ * A delta = r with Jacobi (chebOrder 1) or Chebyshev-Jacobi (chebOrder > 1)
+ * preconditioning on the FP32 coefficients staged last, stopping on
+ * sum|r| <= targetResSum, breakdown, 50 iterations without progress or
+ * maxIter; the minimum-residual iterate is kept.  r is FP64 (host). */
+int cf_pcg(cf_context* ctx, const double* r, double targetResSum,
+           int32_t maxIter, int32_t iterationsPerSync, int32_t chebOrder,
+           double chebBeta, double chebRatio, cf_inner_stats* stats);
+/* metalFoamBackend::bicgstab (metalFoamBackend.H:95-100, .C:735-959) */
+int cf_bicgstab(cf_context* ctx, const double* r, double targetResSum,
+                int32_t maxIter, cf_inner_stats* stats);
+/* metalFoamBackend::delta (metalFoamBackend.H:103): copies the FP32
+ * correction of the last inner solve (caller's cell order). */
+int cf_delta(cf_context* ctx, float* delta);
+
+/* ------------------------------------------------------------ full solve */
+
+/* metalFoamSolver::solveImpl (metalFoamSolver.H:78-85, .C:77-437) with
+ * every FP64 step on the device: residual r = b - A psi, normFactor, the
+ * L1 convergence tests, row sums u = A 1, deflation decision and deflated
+ * diagonal, Gershgorin bound, zero-mean inner right-hand side, psi += delta,
+ * constant-mode shift, hybrid polish.  psi is updated in place.  Uses the
+ * coefficients of the last cf_set_coeffs. */
+int cf_solve(cf_context* ctx, int32_t solver, double* psi,
+             const double* source, const cf_options* opts,
+             cf_performance* perf);
+/* Same with device pointers (psi, source on the context's device). */
+int cf_solve_device(cf_context* ctx, int32_t solver, double* psi,
+                    const double* source, const cf_options* opts,
+                    cf_performance* perf);
+
+/* ------------------------------------------------------------ operators */
+
+/* y = A x in FP64 with lduMatrix::Amul's per-row summation order
+ * (metalFoamSolver.C:109,333); transpose != 0 applies A^T (upper and lower
+ * exchanged).  Host pointers, caller's cell order. */
+int cf_amul(cf_context* ctx, const double* x, double* y, int32_t transpose);
+/* y = A x in FP32 on the staged FP32 coefficients, with the summation
+ * order of the reference's ldu_spmv_dotw kernel
+ * (metalFoamKernels.metal:64-109), and dot = sum w.y (FP64 accumulation).
+ * w may be NULL (dot then not computed). */
+int cf_spmv32(cf_context* ctx, const float* x, const float* w, float* y,
+              double* dot);
+/* z = Chebyshev-Jacobi apply of the given order to r on the spectrum
+ * [beta/ratio, beta] (encCheb, metalFoamBackend.C:342-385), FP32. */
+int cf_cheb_apply(cf_context* ctx, const float* r, float* z, int32_t order,
+                  double beta, double ratio);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,262 @@
+"""ctypes binding of ``libcudafoam.so`` (the C ABI in include/cudafoam.h).
+
+The library is the only compute path: if it is missing or no sm_100 device
+is present, every call raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcudafoam.so")
+
+CF_OK = 0
+STATUS = {
+    0: "CF_OK", 1: "CF_ERR_INVALID_ARG", 2: "CF_ERR_BAD_ADDRESSING", 3: "CF_ERR_NO_TOPOLOGY",
+    4: "CF_ERR_NO_COEFFS", 5: "CF_ERR_CUDA", 6: "CF_ERR_NO_DEVICE", 7: "CF_ERR_DEVICE_TIMEOUT",
+    8: "CF_ERR_UNSUPPORTED", 9: "CF_ERR_TOO_LARGE",
+}
+CF_SOLVER_PCG = 0
+CF_SOLVER_PBICGSTAB = 1
+DEFLATE = {"auto": 0, "on": 1, "off": 2}
+REORDER = {"none": 0, "rcm": 1, "auto": 2}
+
+
+class CudaFoamError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class InnerStats(C.Structure):
+    _fields_ = [
+        ("nIterations", C.c_int32), ("converged", C.c_int32), ("singular", C.c_int32),
+        ("stagnated", C.c_int32), ("finalResSum", C.c_double), ("tGpuSeconds", C.c_double),
+        ("tWallSeconds", C.c_double),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double), ("relTol", C.c_double), ("maxIter", C.c_int32),
+        ("minIter", C.c_int32), ("maxRestarts", C.c_int32), ("iterationsPerSync", C.c_int32),
+        ("deflate", C.c_int32), ("chebyshevOrder", C.c_int32), ("chebyshevRatio", C.c_double),
+        ("profile", C.c_int32), ("verbose", C.c_int32), ("graph", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class Performance(C.Structure):
+    _fields_ = [
+        ("initialResidual", C.c_double), ("finalResidual", C.c_double),
+        ("nIterations", C.c_int32), ("nRestarts", C.c_int32), ("converged", C.c_int32),
+        ("singular", C.c_int32), ("stagnated", C.c_int32), ("deflated", C.c_int32),
+        ("polished", C.c_int32), ("solved", C.c_int32), ("normFactor", C.c_double),
+        ("chebBeta", C.c_double), ("finalResSum32", C.c_double), ("residualL2", C.c_double),
+        ("tConvert", C.c_double), ("tInner", C.c_double), ("tGpu", C.c_double),
+        ("tSolve", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+vp = C.c_void_p
+i32 = C.c_int32
+dbl = C.c_double
+
+# (name, restype, argtypes) of every exported function
+SIGNATURES = [
+    ("cf_abi_version", C.c_int, []),
+    ("cf_last_error", C.c_char_p, []),
+    ("cf_options_default", None, [C.POINTER(Options)]),
+    ("cf_context_create", C.c_int, [C.POINTER(vp), i32]),
+    ("cf_context_destroy", C.c_int, [vp]),
+    ("cf_context_good", C.c_int, [vp]),
+    ("cf_context_description", C.c_char_p, [vp]),
+    ("cf_context_set_stream", C.c_int, [vp, vp]),
+    ("cf_context_set_reorder", C.c_int, [vp, i32]),
+    ("cf_context_kernel_launches", C.c_int, [vp, C.POINTER(C.c_longlong)]),
+    ("cf_set_topology", C.c_int, [vp, i32, i32, vp, vp, vp, vp, vp]),
+    ("cf_set_coeffs", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
+    ("cf_set_coeffs_device", C.c_int, [vp, vp, vp, vp]),
+    ("cf_pcg", C.c_int, [vp, vp, dbl, i32, i32, i32, dbl, dbl, C.POINTER(InnerStats)]),
+    ("cf_bicgstab", C.c_int, [vp, vp, dbl, i32, C.POINTER(InnerStats)]),
+    ("cf_delta", C.c_int, [vp, vp]),
+    ("cf_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
+    ("cf_solve_device", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
+    ("cf_amul", C.c_int, [vp, vp, vp, i32]),
+    ("cf_spmv32", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
+    ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
+]
+
+
+def load():
+    """Load libcudafoam.so (building it first when absent and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise CudaFoamError(6, f"{LIB_PATH} is missing; run python -m metal4foam_b200.build")
+    L = C.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(L, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != CF_OK:
+        msg = load().cf_last_error()
+        raise CudaFoamError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def ptr(a):
+    """Pointer of a C-contiguous numpy array, a torch tensor, or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data_as(vp)
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return vp(a.data_ptr())
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def default_options(**kw):
+    o = Options()
+    load().cf_options_default(C.byref(o))
+    for k, v in kw.items():
+        if k == "deflate" and isinstance(v, str):
+            v = DEFLATE[v]
+        if isinstance(v, bool):
+            v = int(v)
+        if not hasattr(o, k):
+            raise KeyError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+class Context:
+    """One device context = one (mesh, field) backend of the reference
+    (metalFoamSolver::backend(), metalFoamSolver.C:57-74)."""
+
+    def __init__(self, device: int = 0, reorder: str = "auto"):
+        L = load()
+        h = vp()
+        check(L.cf_context_create(C.byref(h), int(device)))
+        self.h = h
+        self._keep = {}
+        check(L.cf_context_set_reorder(self.h, REORDER[reorder]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().cf_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def description(self) -> str:
+        return load().cf_context_description(self.h).decode()
+
+    @property
+    def good(self) -> bool:
+        return bool(load().cf_context_good(self.h))
+
+    def kernel_launches(self) -> int:
+        n = C.c_longlong()
+        check(load().cf_context_kernel_launches(self.h, C.byref(n)))
+        return n.value
+
+    def set_stream(self, stream_handle):
+        check(load().cf_context_set_stream(self.h, vp(stream_handle) if stream_handle else None))
+
+    def set_topology(self, n, nf, low, upp, own, los, losS):
+        arrs = [np.ascontiguousarray(a, np.int32) for a in (low, upp, own, los, losS)]
+        self._keep["topo"] = arrs   # the cache key is the pointer identity
+        check(load().cf_set_topology(self.h, int(n), int(nf), *(ptr(a) for a in arrs)))
+
+    def set_coeffs(self, diag, upper, lower=None):
+        d = np.ascontiguousarray(diag, np.float64)
+        u = np.ascontiguousarray(upper, np.float64)
+        l = None if lower is None else np.ascontiguousarray(lower, np.float64)
+        t = C.c_double()
+        check(load().cf_set_coeffs(self.h, ptr(d), ptr(u), ptr(l), C.byref(t)))
+        return t.value
+
+    def set_coeffs_device(self, diag, upper, lower=None):
+        check(load().cf_set_coeffs_device(self.h, ptr(diag), ptr(upper), ptr(lower)))
+
+    def pcg(self, r, target, maxIter, iterationsPerSync=1, chebOrder=1, chebBeta=2.0,
+            chebRatio=30.0):
+        st = InnerStats()
+        rr = np.ascontiguousarray(r, np.float64)
+        check(load().cf_pcg(self.h, ptr(rr), float(target), int(maxIter),
+                            int(iterationsPerSync), int(chebOrder), float(chebBeta),
+                            float(chebRatio), C.byref(st)))
+        return st
+
+    def bicgstab(self, r, target, maxIter):
+        st = InnerStats()
+        rr = np.ascontiguousarray(r, np.float64)
+        check(load().cf_bicgstab(self.h, ptr(rr), float(target), int(maxIter), C.byref(st)))
+        return st
+
+    def delta(self, n):
+        out = np.empty(n, np.float32)
+        check(load().cf_delta(self.h, ptr(out)))
+        return out
+
+    def solve(self, solver, psi, source, options):
+        perf = Performance()
+        check(load().cf_solve(self.h, int(solver), ptr(psi), ptr(source), C.byref(options),
+                              C.byref(perf)))
+        return perf
+
+    def solve_device(self, solver, psi, source, options):
+        perf = Performance()
+        check(load().cf_solve_device(self.h, int(solver), ptr(psi), ptr(source),
+                                     C.byref(options), C.byref(perf)))
+        return perf
+
+    def amul(self, x, transpose=False):
+        xx = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(xx)
+        check(load().cf_amul(self.h, ptr(xx), ptr(y), int(transpose)))
+        return y
+
+    def spmv32(self, x, w=None):
+        xx = np.ascontiguousarray(x, np.float32)
+        ww = None if w is None else np.ascontiguousarray(w, np.float32)
+        y = np.empty_like(xx)
+        d = C.c_double()
+        check(load().cf_spmv32(self.h, ptr(xx), ptr(ww), ptr(y), C.byref(d)))
+        return y, d.value
+
+    def cheb_apply(self, r, order, beta, ratio=30.0):
+        rr = np.ascontiguousarray(r, np.float32)
+        z = np.empty_like(rr)
+        check(load().cf_cheb_apply(self.h, ptr(rr), ptr(z), int(order), float(beta),
+                                   float(ratio)))
+        return z

@@ -1,0 +1,110 @@
+// cf_host.hpp -- the context object behind the opaque cf_context handle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "cf_internal.cuh"
+#include "cf_kernels.cuh"
+
+constexpr int CF_MAX_CHEB = 64;
+
+struct cf_context
+{
+    // device / runtime (metalFoamBackend::Impl::init, metalFoamBackend.C:192-282)
+    int device = 0;
+    int numSMs = 1;
+    int maxBlocksPerSM = 8;
+    int l2Bytes = 0;
+    bool good = false;
+    std::string description = "cudaFoam: no device";
+    cudaStream_t ownStream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+    std::map<const void*, int> occ;        // kernel -> resident blocks per SM
+    long long launches = 0;                // kernels launched (graph bodies counted per pass)
+
+    // topology (metalFoamBackend::setTopology, .C:454-519)
+    bool hasTopo = false;
+    int reorderMode = 2;                   // CF_REORDER_AUTO
+    int topoReorderMode = -1;
+    int n = 0, nf = 0, nslices = 0, maxRowLen = 0;
+    long long nnzp = 0;
+    const int32_t* lastLow = nullptr;
+    const int32_t* lastUpp = nullptr;
+    std::vector<int32_t> perm;             // internal row -> caller's cell
+    bool identityPerm = true;
+    std::vector<void*> topoAllocs;
+    int* d_sliceOff = nullptr;
+    int* d_col = nullptr;
+    int* d_eface = nullptr;
+    int* d_perm = nullptr;
+    int* d_low = nullptr;
+    int* d_upp = nullptr;
+
+    // coefficients (metalFoamBackend::setCoeffs, .C:522-565)
+    bool hasCoeffs = false;
+    bool hasLower = false;
+    int val32Sym = 1;
+    double* d_diagIn = nullptr;            // caller's order
+    double* d_upper = nullptr;             // face order
+    double* d_lower = nullptr;
+    double* d_diag64 = nullptr;            // internal order
+    double* d_u = nullptr;                 // row sums A 1
+    float* d_val32 = nullptr;
+    double* d_val64 = nullptr;
+    double* d_valT64 = nullptr;
+    float* d_diag32 = nullptr;
+    float* d_rD32 = nullptr;
+
+    // vectors (internal order)
+    double* d_psi = nullptr;
+    double* d_b = nullptr;
+    double* d_r64 = nullptr;
+    double* d_io64 = nullptr;              // staging for caller-order FP64 data
+    double* d_io64b = nullptr;
+    float* d_rA = nullptr;
+    float* d_W0 = nullptr;
+    float* d_W1 = nullptr;
+    float* d_Z0 = nullptr;
+    float* d_Z1 = nullptr;
+    float* d_P = nullptr;                  // 2n
+    float* d_Q = nullptr;
+    float* d_T = nullptr;
+    float* d_D = nullptr;                  // 3n
+    float* d_io32 = nullptr;
+    float* d_io32b = nullptr;
+    float* d_io32c = nullptr;
+
+    // scalars
+    double* d_part = nullptr;
+    cf::InnerState* d_st = nullptr;
+    cf::DriverState* d_drv = nullptr;
+    float* d_chebC = nullptr;
+    double* d_scratch64 = nullptr;
+    cf::InnerState* h_st = nullptr;        // pinned mirrors
+    cf::DriverState* h_drv = nullptr;
+    int lastInnerKind = -1;                // 0 pcg, 1 bicgstab (for cf_delta)
+    int pendingBodyKernels = 0;            // kernels per graph-body pass of the last inner solve
+
+    // instantiated inner-loop graphs keyed by (kind, chebyshev order)
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+};
+
+namespace cf {
+
+int fail(int code, const std::string& msg);
+double wall_now();
+int grid_for(cf_context* c, const void* fn, long long work);
+DevSell sell_of(const cf_context* c);
+PcgBufs pcg_bufs(const cf_context* c);
+BicgBufs bicg_bufs(const cf_context* c);
+int stage_vals(cf_context* c, int sym32);
+int stage_diag32(cf_context* c, int deflate);
+
+}  // namespace cf
