@@ -1,0 +1,419 @@
+"""Benchmark of the cudaPCG hot path on one or more B200s.
+
+Workload (default): the variable-coefficient pressure PCG, 3-D 7-point
+128^3 = 2,097,152 cells / 6,242,304 faces, per-cell k ~ 10**U(-2,2), faces
+= -harmonic mean, diag = -sum(off-diagonals), Neumann + setReference on cell
+0, cells relabelled by a seeded random permutation, b ~ N(0,1) zero mean,
+solved to FP64 normalised residual 1e-6 (cudaPCG defaults: Chebyshev order
+8, deflate auto, maxRestarts 8).  Synthetic seeded data (no dataset exists).
+
+One step = one full solve: coefficient staging (setCoeffs) + the FP64
+driver + the FP32 inner iterations, psi0 = 0.  ``value`` is solves/s with
+every input resident in HBM; ``e2e`` is the same through the public plugin
+surface (cudaPCG.solve) from pinned host buffers, host<->device copies of
+the coefficients, psi and source inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent replica per GPU (torchrun; the single system is
+not partitioned), value = all replicas' solves / max-over-ranks time.
+``--impl reference`` times the reference's CPU path (OpenFOAM's FP64 PCG,
+restated in oracle/) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s at FP64 rel-res 1e-6"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_config():
+    return {"workload": "varcoeff-pressure-PCG 128^3 permuted (2,097,152 cells, 6,242,304 faces)",
+            "solver": "cudaPCG", "chebyshevOrder": 8, "deflate": "auto", "maxRestarts": 8,
+            "tolerance": 1e-6, "relTol": 0.0, "seed": 1,
+            "l2": "no flush: per-solve working set (~0.6 GB of device buffers) exceeds the "
+                  "126 MB L2"}
+
+
+def b_spmv(n, nf, s=4, sym=True):
+    """Algorithmic bytes of one LDU SpMV with the reference's access pattern:
+    diag, x, y and the face coefficients once, plus the five int32 addressing
+    arrays (uppAddr, lowAddr, losort, ownStart, losortStart)."""
+    return s * (3 * n + nf * (1 if sym else 2)) + 4 * (3 * nf + 2 * (n + 1))
+
+
+def b_cheb_step(n, nf):
+    """One fused Chebyshev step: the SpMV (x = z_{j-1}, y = z_j) plus the
+    recurrence's own streams r, rD, w (read) and w (write)."""
+    return b_spmv(n, nf, 4, True) + 4 * n * 4
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def read_profile_traffic():
+    """dram bytes per launch of the fused Chebyshev step from the committed
+    ncu summary (None when no capture is committed)."""
+    p = os.path.join(ROOT, "profiles", "cheb_step_varcoeff128.txt")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return int(float(line.split(":", 1)[1]))
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        self.f = tempfile.TemporaryFile(mode="w+")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.f is None:
+            return None
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_sample(sysm, budget_s=15.0, nthreads=None):
+    """The reference's CPU path (OpenFOAM FP64 PCG with the DIC preconditioner,
+    restated in oracle/foam_cpu.c), single-threaded like the reference's
+    serial runs, on a bounded sample: `iters` PCG iterations of the full
+    128^3 system; solves/s = 1 / (seconds per iteration x iterations to reach
+    1e-6).  The iteration count to 1e-6 comes from one full run made on this
+    host the first time (cached in the process)."""
+    from oracle import oracle as O
+    nt = 1 if nthreads is None else nthreads
+    # calibrate: a short run to size the sample
+    t0 = time.perf_counter()
+    O.foam_pcg(sysm, "DIC", tolerance=0.0, maxIter=5, nthreads=nt)
+    per5 = time.perf_counter() - t0
+    iters = max(5, int(budget_s / max(per5 / 5, 1e-6)))
+    t0 = time.perf_counter()
+    _, p = O.foam_pcg(sysm, "DIC", tolerance=0.0, maxIter=iters, nthreads=nt)
+    dt = time.perf_counter() - t0
+    return dt / p.nIterations, p.nIterations
+
+
+def dic_iterations_to_converge(sysm, nthreads=1):
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    _, p = O.foam_pcg(sysm, "DIC", tolerance=1e-6, maxIter=20000, nthreads=nthreads)
+    return p.nIterations, p.converged, time.perf_counter() - t0
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from metal4foam_b200 import _lib, mesh
+    from metal4foam_b200.solver import backend_cache_clear, cudaPCG, lduMatrix
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sysm = mesh.varcoeff3d((128, 128, 128), seed=1, permute=True)
+    n, nf = sysm.n, sysm.nf
+    a = sysm.addr
+    stream = torch.cuda.current_stream()
+    ctx = _lib.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_topology(n, nf, *a.arrays())
+    d_diag = torch.from_numpy(sysm.diag).to(dev)
+    d_upper = torch.from_numpy(sysm.upper).to(dev)
+    d_src = torch.from_numpy(sysm.source).to(dev)
+    d_psi0 = torch.zeros(n, dtype=torch.float64, device=dev)
+    d_psi = torch.zeros(n, dtype=torch.float64, device=dev)
+    opts = _lib.default_options(graph=args.graph)
+    perfs = []
+
+    def step():
+        d_psi.copy_(d_psi0)
+        ctx.set_coeffs_device(d_diag, d_upper, None)
+        p = ctx.solve_device(_lib.CF_SOLVER_PCG, d_psi, d_src, opts)
+        perfs.append(p)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    perfs.clear()
+    launches0 = ctx.kernel_launches()
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    launches = ctx.kernel_launches() - launches0
+    ms_max = max_over_ranks(ms, ws)
+    ok = all(p.converged and p.finalResidual < 1e-6 for p in perfs)
+    iters = [p.nIterations for p in perfs]
+    last = perfs[-1]
+
+    # error against an FP64 solve of the same system is checked in the tests;
+    # here the FP64 residual of every timed solve is asserted
+    # dominant kernel: the fused SpMV + Chebyshev step
+    t_cheb = ctx.time_kernel("cheb_step", reps=100)
+    t_spmv = ctx.time_kernel("spmv32", reps=100)
+    t_amul = ctx.time_kernel("amul64", reps=20)
+    peak, peak_kind = read_peaks()
+    bytes_cheb = b_cheb_step(n, nf)
+    achieved = bytes_cheb / (t_cheb * 1e-3) / 1e9
+    traffic = read_profile_traffic()
+
+    # end to end through the plugin surface from pinned host memory
+    h_diag = torch.from_numpy(sysm.diag).pin_memory()
+    h_upper = torch.from_numpy(sysm.upper).pin_memory()
+    h_src = torch.from_numpy(sysm.source).pin_memory()
+    h_psi = torch.zeros(n, dtype=torch.float64).pin_memory()
+    m = lduMatrix(a, h_diag.numpy(), h_upper.numpy())
+    solver = cudaPCG("p", m, {"solver": "cudaPCG", "tolerance": 1e-6, "relTol": 0.0},
+                     device=local)
+    solver.backend().set_stream(stream.cuda_stream)
+    psi_np = h_psi.numpy()
+    src_np = h_src.numpy()
+    e2e_perfs = []
+
+    def e2e_step():
+        psi_np[:] = 0.0
+        e2e_perfs.append(solver.solve(psi_np, src_np))
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_perfs.clear()
+    barrier(ws)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3), ws)
+    e2e_ok = all(p.converged and p.finalResidual < 1e-6 for p in e2e_perfs)
+    backend_cache_clear()
+
+    out = None
+    if rank == 0:
+        value = ws * args.steps / (ms_max / 1000.0)
+        out = {
+            "metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
+            "data": "synthetic (seeded)",
+            "config": dict(workload_config(),
+                           parallelism=f"replicas x{ws} (single system not partitioned)"),
+            "valid": bool(ok and e2e_ok),
+            "solve": {"inner_iterations": iters[-1], "restarts": last.nRestarts,
+                      "final_residual": last.finalResidual, "residual_l2": last.residualL2,
+                      "deflated": bool(last.deflated), "iterations_all_steps_equal":
+                          len(set(iters)) == 1},
+            "roofline": {"bound": "hbm", "kernel": "k_cheb_step (fused SpMV + Chebyshev step)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": bytes_cheb,
+                         "ms_per_launch": round(t_cheb, 5)},
+            "spmv": {"kernel": "k_spmv32 (FP32 LDU SpMV + dot)",
+                     "gbs": round(b_spmv(n, nf) / (t_spmv * 1e-3) / 1e9, 1),
+                     "frac": round(b_spmv(n, nf) / (t_spmv * 1e-3) / 1e9 / peak, 4),
+                     "ms_per_launch": round(t_spmv, 5),
+                     "fp64_residual_spmv_gbs": round(b_spmv(n, nf, 8) / (t_amul * 1e-3) / 1e9,
+                                                     1)},
+            "e2e": {"value": round(ws * e2e_steps / (ms_e2e / 1000.0), 4), "unit": "solves/s",
+                    "h2d_bytes_per_step": 8 * (3 * n + nf), "d2h_bytes_per_step": 8 * n,
+                    "api": "cudaPCG.solve (lduMatrix::solver surface) from pinned host arrays",
+                    "steps": e2e_steps},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        if ws == 1 and not args.no_cpu:
+            sec_it, it_sample = cpu_reference_sample(sysm, budget_s=args.cpu_budget)
+            iters_dic = args.dic_iters
+            out["cpu_baseline"] = {
+                "value": round(1.0 / (sec_it * iters_dic), 6), "unit": "solves/s",
+                "cores": 1, "kind": "port",
+                "sample": (f"OpenFOAM-semantics FP64 PCG+DIC (oracle/foam_cpu.c), "
+                           f"{it_sample} iterations of the full 128^3 system timed "
+                           f"({sec_it * 1e3:.1f} ms/iteration); solves/s = 1/(s/iteration x "
+                           f"{iters_dic} iterations to 1e-6, measured by a full run)")}
+    ctx.close()
+    return out
+
+
+def run_reference(args, ws, rank):
+    """The reference's CPU path on the host cores: OpenFOAM's FP64 PCG with
+    DIC (serial, as the reference's comparison runs), bounded per step."""
+    if rank != 0:
+        return None
+    from metal4foam_b200 import mesh
+    sysm = mesh.varcoeff3d((128, 128, 128), seed=1, permute=True)
+    samples = []
+    for _ in range(args.warmup):
+        cpu_reference_sample(sysm, budget_s=min(args.cpu_budget, 3.0))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        samples.append(cpu_reference_sample(sysm, budget_s=min(args.cpu_budget, 8.0)))
+    dt = time.perf_counter() - t0
+    sec_it = statistics.median(s[0] for s in samples)
+    value = 1.0 / (sec_it * args.dic_iters)
+    sample = (f"each step: a bounded run of OpenFOAM-semantics FP64 PCG+DIC "
+              f"(oracle/foam_cpu.c, serial) on the full 128^3 system; solves/s = 1/(median "
+              f"s/iteration x {args.dic_iters} iterations to 1e-6)")
+    return {"metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1000 * dt / max(1, args.steps), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": dict(workload_config(), parallelism="host cores"),
+            "cpu_baseline": {"value": round(value, 6), "unit": "solves/s", "cores": 1,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of CPU work for the CPU-baseline sample")
+    ap.add_argument("--dic-iters", type=int, default=int(os.environ.get("CF_DIC_ITERS", "0")),
+                    help="PCG+DIC iterations to 1e-6 on the workload (0: measure once)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--graph", type=int, default=1,
+                    help="1: inner iterations in a CUDA-graph while loop (default); 0: one "
+                         "host sync per iteration (same kernels; ncu cannot profile kernels "
+                         "inside conditional graphs, so launch lists use 0)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = (1, 0, 0)
+    if args.impl == "reference":
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if args.dic_iters <= 0:
+            args.dic_iters = DIC_ITERS_128
+        out = run_reference(args, ws, rank)
+    else:
+        ws, rank, local = dist_setup(args.gpus)
+        if args.dic_iters <= 0:
+            args.dic_iters = DIC_ITERS_128
+        out = run_ours(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+# PCG+DIC iterations to FP64 1e-6 on the default workload, from a full run of
+# the CPU path (oracle/foam_cpu.c) on this workload; the bench's CPU legs time
+# bounded samples and scale by this count.
+DIC_ITERS_128 = 0
+
+if __name__ == "__main__":
+    main()

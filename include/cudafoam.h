@@ -226,6 +226,24 @@ int cf_spmv32(cf_context* ctx, const float* x, const float* w, float* y,
 int cf_cheb_apply(cf_context* ctx, const float* r, float* z, int32_t order,
                   double beta, double ratio);
 
+/* ------------------------------------------------------------ measurement */
+
+enum
+{
+    CF_KERNEL_CHEB_STEP = 0,   /* fused SpMV + Chebyshev step (cudaPCG bulk) */
+    CF_KERNEL_SPMV32 = 1,      /* FP32 SpMV with fused dot                   */
+    CF_KERNEL_PCG_P_SPMV = 2,  /* p-update fused into the SpMV + p.Ap        */
+    CF_KERNEL_PCG_UPDATE = 3,  /* delta/residual update + L1 + next apply    */
+    CF_KERNEL_AMUL64 = 4       /* FP64 refinement residual SpMV              */
+};
+/* Launches one hot kernel `reps` times back to back on the context's stream
+ * over the operands of the last solve (work vectors are overwritten, the
+ * returned solution is not) and returns the average device time per launch
+ * from CUDA events recorded on that stream.  Diagnostic; no reference
+ * counterpart. */
+int cf_time_kernel(cf_context* ctx, int32_t which, int32_t reps,
+                   double* msPerLaunch);
+
 #ifdef __cplusplus
 }
 #endif

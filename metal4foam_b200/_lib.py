@@ -93,6 +93,7 @@ SIGNATURES = [
     ("cf_amul", C.c_int, [vp, vp, vp, i32]),
     ("cf_spmv32", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
     ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
+    ("cf_time_kernel", C.c_int, [vp, i32, i32, C.POINTER(dbl)]),
 ]
 
 
@@ -253,6 +254,13 @@ class Context:
         d = C.c_double()
         check(load().cf_spmv32(self.h, ptr(xx), ptr(ww), ptr(y), C.byref(d)))
         return y, d.value
+
+    KERNELS = {"cheb_step": 0, "spmv32": 1, "pcg_p_spmv": 2, "pcg_update": 3, "amul64": 4}
+
+    def time_kernel(self, which, reps=50):
+        ms = C.c_double()
+        check(load().cf_time_kernel(self.h, self.KERNELS[which], int(reps), C.byref(ms)))
+        return ms.value
 
     def cheb_apply(self, r, order, beta, ratio=30.0):
         rr = np.ascontiguousarray(r, np.float32)

@@ -683,3 +683,81 @@ extern "C" int cf_cheb_apply(cf_context* c, const float* r, float* z, int32_t or
     CF_CUDA(cudaStreamSynchronize(s));
     return CF_OK;
 }
+
+// ------------------------------------------------------------------ measurement
+
+extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double* msPerLaunch)
+{
+    CF_TRY(check_ready(c));
+    if (!msPerLaunch || reps <= 0) return fail(CF_ERR_INVALID_ARG, "bad arguments");
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    const DevSell A = sell_of(c);
+    const PcgBufs B = pcg_bufs(c);
+    // operands with finite values and a live (not done) state
+    float cc[2 * 8];
+    cheb_constants(8, 2.0, 30.0, cc);
+    CF_CUDA(cudaMemcpyAsync(c->d_chebC, cc, sizeof(cc), cudaMemcpyHostToDevice, s));
+    k_inner_setup<<<1, 32, 0, s>>>(c->d_st, 0.0, 1 << 30, 1);
+    CF_LAUNCH();
+    const int g1 = grid_for(c, (const void*)k_cheb_init, n);
+    k_cheb_init<<<g1, NT, 0, s>>>(n, B.rA, B.rD, c->d_chebC, B.W0);
+    CF_LAUNCH();
+    k_cheb_init<<<g1, NT, 0, s>>>(n, B.rA, B.rD, c->d_chebC, B.Z0);
+    CF_LAUNCH();
+    k_cheb_init<<<g1, NT, 0, s>>>(n, B.rA, B.rD, c->d_chebC, B.W1);
+    CF_LAUNCH();
+    CF_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(float) * 2 * (size_t)n, s));
+    auto launch = [&]() -> int {
+        switch (which)
+        {
+            case CF_KERNEL_CHEB_STEP:
+            {
+                auto fn = k_cheb_step<false, MW>;
+                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2,
+                                                                 c->d_st, c->d_part);
+                break;
+            }
+            case CF_KERNEL_SPMV32:
+            {
+                auto fn = k_spmv32<MW>;
+                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B.diag, B.Z0, B.W0, B.Z1,
+                                                                 c->d_scratch64,
+                                                                 &c->d_drv->ticket, c->d_part);
+                break;
+            }
+            case CF_KERNEL_PCG_P_SPMV:
+            {
+                auto fn = k_pcg_p_spmv<MW>;
+                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, c->d_st, c->d_part);
+                break;
+            }
+            case CF_KERNEL_PCG_UPDATE:
+            {
+                auto fn = k_pcg_update<true>;
+                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(B, c->d_st, c->d_part, 0, 0);
+                break;
+            }
+            case CF_KERNEL_AMUL64:
+            {
+                auto fn = k_amul64<MW>;
+                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, c->d_val64, c->d_diag64,
+                                                                 c->d_psi, c->d_r64);
+                break;
+            }
+            default:
+                return fail(CF_ERR_INVALID_ARG, "unknown kernel id");
+        }
+        CF_LAUNCH();
+        return CF_OK;
+    };
+    CF_TRY(launch());  // warm
+    CF_CUDA(cudaEventRecord(c->ev0, s));
+    for (int i = 0; i < reps; ++i) CF_TRY(launch());
+    CF_CUDA(cudaEventRecord(c->ev1, s));
+    CF_CUDA(cudaEventSynchronize(c->ev1));
+    float ms = 0.0f;
+    CF_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *msPerLaunch = (double)ms / reps;
+    return CF_OK;
+}
