@@ -208,6 +208,10 @@ int cf_solve(cf_context* ctx, int32_t solver, double* psi,
 int cf_solve_device(cf_context* ctx, int32_t solver, double* psi,
                     const double* source, const cf_options* opts,
                     cf_performance* perf);
+/* FP64 residual field b - A psi of the last cf_solve (which = 0: at entry,
+ * 1: at exit), caller's cell order, for lduMatrix::setResidualField
+ * (metalFoamSolver.C:112-117,429-434). */
+int cf_residual(cf_context* ctx, int32_t which, double* r);
 
 /* ------------------------------------------------------------ operators */
 

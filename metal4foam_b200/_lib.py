@@ -90,6 +90,7 @@ SIGNATURES = [
     ("cf_delta", C.c_int, [vp, vp]),
     ("cf_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_solve_device", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
+    ("cf_residual", C.c_int, [vp, i32, vp]),
     ("cf_amul", C.c_int, [vp, vp, vp, i32]),
     ("cf_spmv32", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
     ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
@@ -240,6 +241,11 @@ class Context:
         check(load().cf_solve_device(self.h, int(solver), ptr(psi), ptr(source),
                                      C.byref(options), C.byref(perf)))
         return perf
+
+    def residual(self, n, which="final"):
+        out = np.empty(n)
+        check(load().cf_residual(self.h, {"initial": 0, "final": 1}[which], ptr(out)))
+        return out
 
     def amul(self, x, transpose=False):
         xx = np.ascontiguousarray(x, np.float64)

@@ -528,6 +528,8 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
     CF_TRY(dalloc(c, &c->d_r64, N));
     CF_TRY(dalloc(c, &c->d_io64, N));
     CF_TRY(dalloc(c, &c->d_io64b, N));
+    CF_TRY(dalloc(c, &c->d_r0, N));
+    c->hasResidual = false;
     CF_TRY(dalloc(c, &c->d_rA, N));
     CF_TRY(dalloc(c, &c->d_W0, N));
     CF_TRY(dalloc(c, &c->d_W1, N));

@@ -68,6 +68,8 @@ struct cf_context
     double* d_r64 = nullptr;
     double* d_io64 = nullptr;              // staging for caller-order FP64 data
     double* d_io64b = nullptr;
+    double* d_r0 = nullptr;                // residual at the entry of the last solve
+    bool hasResidual = false;
     float* d_rA = nullptr;
     float* d_W0 = nullptr;
     float* d_W1 = nullptr;

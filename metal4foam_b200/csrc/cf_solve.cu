@@ -355,7 +355,9 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
                                                          c->d_r64, c->d_drv, c->d_part);
         CF_LAUNCH();
     }
+    CF_CUDA(cudaMemcpyAsync(c->d_r0, c->d_r64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     CF_TRY(fetch_drv(c));
+    c->hasResidual = true;
     perf->normFactor = c->h_drv->normFactor;
     perf->initialResidual = c->h_drv->initRes;
     perf->finalResidual = perf->initialResidual;
@@ -581,6 +583,20 @@ extern "C" int cf_solve(cf_context* c, int32_t solver, double* psi, const double
     CF_TRY(solve_device(c, solver, c->d_io64, c->d_io64b, o, perf));
     CF_CUDA(cudaMemcpyAsync(psi, c->d_io64, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
                             c->stream));
+    CF_CUDA(cudaStreamSynchronize(c->stream));
+    return CF_OK;
+}
+
+extern "C" int cf_residual(cf_context* c, int32_t which, double* r)
+{
+    CF_TRY(check_ready(c));
+    if (!r || (which != 0 && which != 1)) return fail(CF_ERR_INVALID_ARG, "bad arguments");
+    if (!c->hasResidual) return fail(CF_ERR_INVALID_ARG, "no solve has run on this context");
+    const int n = c->n;
+    k_scatter_f64<<<grid_for(c, (const void*)k_scatter_f64, n), NT, 0, c->stream>>>(
+        n, c->d_perm, which == 0 ? c->d_r0 : c->d_r64, c->d_io64b);
+    CF_LAUNCH();
+    CF_CUDA(cudaMemcpyAsync(r, c->d_io64b, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
     CF_CUDA(cudaStreamSynchronize(c->stream));
     return CF_OK;
 }

@@ -188,6 +188,33 @@ def permute_cells(newlabel: np.ndarray, low, upp, *face_arrays):
     return out
 
 
+def relabel(sysm: LduSystem, seed: int) -> LduSystem:
+    """The same linear system with cells renumbered by a seeded permutation
+    (faces re-oriented and re-sorted into LDU order; an asymmetric face whose
+    owner and neighbour swap also swaps its upper/lower coefficients)."""
+    rng = np.random.default_rng(seed)
+    nl = rng.permutation(sysm.n)
+    a = sysm.addr
+    lo = nl[a.lowerAddr]
+    hi = nl[a.upperAddr]
+    swap = lo > hi
+    lower = sysm.lower_or_upper
+    up = np.where(swap, lower, sysm.upper)
+    lw = np.where(swap, sysm.upper, lower)
+    L = np.minimum(lo, hi)
+    H = np.maximum(lo, hi)
+    o = np.lexsort((H, L))
+    addr = ldu_addressing(sysm.n, L[o], H[o])
+    diag = np.empty(sysm.n)
+    diag[nl] = sysm.diag
+    src = np.empty(sysm.n)
+    src[nl] = sysm.source
+    psi = np.empty(sysm.n)
+    psi[nl] = sysm.psi
+    return LduSystem(sysm.name + f"_relabel{seed}", addr, diag, up[o],
+                     None if sysm.lower is None else lw[o], src, psi, dict(sysm.meta))
+
+
 def poisson2d(nx: int = 128, ny: int = 128, seed: int = 0) -> LduSystem:
     """2-D 5-point Neumann Poisson with setReference on cell 0.
 

@@ -1,0 +1,242 @@
+/*---------------------------------------------------------------------------*\
+    cudaFoam: B200 (sm_100a) Krylov solvers for OpenFOAM lduMatrix systems
+
+    Driver of cudaPCG / cudaPBiCGStab over libcudafoam.so.  Same controls,
+    same residual definitions and the same fatal errors as metal4Foam's
+    metalFoamSolver (src/metal4Foam/solvers/metalFoamSolver.C:32-437); the
+    FP64 steps that file runs on the CPU run inside cf_solve on the device.
+\*---------------------------------------------------------------------------*/
+
+#include "cudaFoamSolver.H"
+#include "PrecisionAdaptor.H"
+#include "cudafoam.h"
+
+#include <fenv.h>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+
+static_assert
+(
+    sizeof(Foam::solveScalar) == 8,
+    "cudaFoam requires a double-precision (WM_PRECISION_OPTION=DP) build"
+);
+static_assert
+(
+    sizeof(Foam::label) == 4,
+    "cudaFoam requires a 32-bit label (WM_LABEL_SIZE=32) build"
+);
+
+namespace
+{
+
+// OpenFOAM traps SIGFPE; driver and runtime code may raise FP exceptions
+// legitimately.  Run every library call with the default FP environment and
+// restore the caller's afterwards (per thread).
+struct FpTrapGuard
+{
+    fenv_t saved;
+    FpTrapGuard() { fegetenv(&saved); fesetenv(FE_DFL_ENV); }
+    ~FpTrapGuard() { fesetenv(&saved); }
+};
+
+struct ContextDeleter
+{
+    void operator()(cf_context* c) const { cf_context_destroy(c); }
+};
+
+int deflateMode(const Foam::word& w)
+{
+    if (w == "on") return CF_DEFLATE_ON;
+    if (w == "off") return CF_DEFLATE_OFF;
+    if (w == "auto") return CF_DEFLATE_AUTO;
+    FatalErrorInFunction
+        << "deflate must be on, off or auto, not " << w << Foam::exit(Foam::FatalError);
+    return CF_DEFLATE_AUTO;
+}
+
+} // anonymous namespace
+
+
+Foam::cudaFoamSolver::cudaFoamSolver
+(
+    const word& fieldName,
+    const lduMatrix& matrix,
+    const FieldField<Field, scalar>& interfaceBouCoeffs,
+    const FieldField<Field, scalar>& interfaceIntCoeffs,
+    const lduInterfaceFieldPtrsList& interfaces,
+    const dictionary& solverControls
+)
+:
+    lduMatrix::solver
+    (
+        fieldName,
+        matrix,
+        interfaceBouCoeffs,
+        interfaceIntCoeffs,
+        interfaces,
+        solverControls
+    ),
+    cudaDict_
+    (
+        solverControls.found("cuda")
+      ? solverControls.subDict("cuda")
+      : solverControls.subOrEmptyDict("metal")
+    )
+{}
+
+
+cf_context* Foam::cudaFoamSolver::backend() const
+{
+    // The solver object is rebuilt on every fvMatrix::solve: keep one device
+    // context per (field, mesh) for the run, as the reference does.
+    static std::map<std::string, std::unique_ptr<cf_context, ContextDeleter>> cache;
+
+    std::ostringstream key;
+    key << fieldName_ << '@' << static_cast<const void*>(&matrix_.mesh());
+    auto& slot = cache[key.str()];
+    if (!slot)
+    {
+        FpTrapGuard fpe;
+        cf_context* c = nullptr;
+        if (cf_context_create(&c, 0) != CF_OK)
+        {
+            FatalErrorInFunction
+                << "CUDA backend unavailable: " << cf_last_error()
+                << exit(FatalError);
+        }
+        slot.reset(c);
+        Info<< "    " << cf_context_description(c) << nl;
+    }
+    return slot.get();
+}
+
+
+Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
+(
+    const word& solverName,
+    const bool useBiCGStab,
+    solveScalarField& psi,
+    const solveScalarField& source,
+    const direction cmpt
+) const
+{
+    // Coupled interfaces (processor/cyclic/AMI) cannot be applied inside the
+    // device-resident iteration.
+    forAll(interfaces_, patchi)
+    {
+        if (interfaces_.set(patchi))
+        {
+            FatalErrorInFunction
+                << solverName << " does not support coupled boundaries "
+                << "(processor/cyclic/AMI); run serially on a mesh "
+                << "without coupled patches."
+                << exit(FatalError);
+        }
+    }
+
+    solverPerformance solverPerf(solverName, fieldName_);
+    cf_context* ctx = backend();
+    FpTrapGuard fpe;
+
+    const lduAddressing& addr = matrix_.mesh().lduAddr();
+    const label nCells = addr.size();
+    const label nFaces = addr.upperAddr().size();
+
+    auto check = [&](int rc, const char* what)
+    {
+        if (rc != CF_OK)
+        {
+            FatalErrorInFunction
+                << solverName << ": " << what << " failed: " << cf_last_error()
+                << exit(FatalError);
+        }
+    };
+
+    check
+    (
+        cf_set_topology
+        (
+            ctx, nCells, nFaces,
+            addr.lowerAddr().cdata(),
+            addr.upperAddr().cdata(),
+            addr.ownerStartAddr().cdata(),
+            addr.losortAddr().cdata(),
+            addr.losortStartAddr().cdata()
+        ),
+        "cf_set_topology"
+    );
+    double tConvert = 0;
+    check
+    (
+        cf_set_coeffs
+        (
+            ctx,
+            matrix_.diag().cdata(),
+            matrix_.upper().cdata(),
+            matrix_.hasLower() ? matrix_.lower().cdata() : nullptr,
+            &tConvert
+        ),
+        "cf_set_coeffs"
+    );
+
+    cf_options opts;
+    cf_options_default(&opts);
+    opts.tolerance = tolerance_;
+    opts.relTol = relTol_;
+    opts.maxIter = maxIter_;
+    opts.minIter = minIter_;
+    opts.maxRestarts = cudaDict_.getOrDefault<label>("maxRestarts", 8);
+    opts.iterationsPerSync = cudaDict_.getOrDefault<label>("iterationsPerSync", 1);
+    opts.deflate = deflateMode(cudaDict_.getOrDefault<word>("deflate", "auto"));
+    opts.chebyshevOrder = cudaDict_.getOrDefault<label>("chebyshevOrder", 8);
+    opts.chebyshevRatio = cudaDict_.getOrDefault<scalar>("chebyshevRatio", 30.0);
+    opts.profile = cudaDict_.getOrDefault<bool>("profile", false);
+    opts.verbose = cudaDict_.getOrDefault<bool>("verbose", false);
+    opts.graph = cudaDict_.getOrDefault<bool>("graph", true);
+
+    cf_performance perf;
+    check
+    (
+        cf_solve
+        (
+            ctx,
+            useBiCGStab ? CF_SOLVER_PBICGSTAB : CF_SOLVER_PCG,
+            psi.data(),
+            source.cdata(),
+            &opts,
+            &perf
+        ),
+        "cf_solve"
+    );
+
+    solverPerf.initialResidual() = perf.initialResidual;
+    solverPerf.finalResidual() = perf.finalResidual;
+    solverPerf.nIterations() = perf.nIterations;
+    solverPerf.checkConvergence(tolerance_, relTol_, log_);
+    if (perf.singular)
+    {
+        solverPerf.checkSingularity(0);
+    }
+
+    // residual fields at entry and exit, as metalFoamSolver.C:112-117,429-434
+    solveScalarField rA(nCells);
+    check(cf_residual(ctx, 0, rA.data()), "cf_residual");
+    matrix().setResidualField
+    (
+        ConstPrecisionAdaptor<scalar, solveScalar>(rA)(), fieldName_, true
+    );
+    check(cf_residual(ctx, 1, rA.data()), "cf_residual");
+    matrix().setResidualField
+    (
+        ConstPrecisionAdaptor<scalar, solveScalar>(rA)(), fieldName_, false
+    );
+
+    if (opts.profile)
+    {
+        Info<< "    " << solverName << " profile: tConvert=" << 1000*tConvert
+            << "ms" << nl;
+    }
+    return solverPerf;
+}

