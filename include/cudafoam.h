@@ -248,6 +248,37 @@ enum
 int cf_time_kernel(cf_context* ctx, int32_t which, int32_t reps,
                    double* msPerLaunch);
 
+/* ------------------------------------------------------------ no allocation */
+
+/* y = A x and *dot = sum w.y for callers that cannot allocate device memory:
+ * code running inside someone else's CUDA-graph capture, solver threads
+ * that must not take the allocator's locks, or frameworks that hand out only
+ * their own pre-allocated buffers.  No counterpart in the reference.
+ *
+ * Everything is a device pointer on the current device and is owned by the
+ * caller: the LDU arrays as cf_set_topology takes them, FP32 coefficients
+ * (lower NULL: symmetric), x, w (NULL: dot = 0), y and dot (one double;
+ * NULL: no dot).  The row sums use the reference kernel's order (diagonal,
+ * owner-side faces, then losort faces).  The call is asynchronous on
+ * `stream` (a cudaStream_t, NULL: the default stream) and calls no
+ * cudaMalloc, cudaFree or allocating library routine: the per-block
+ * partial sums live in a fixed file-scope device array of 65,536 doubles
+ * plus one 256-byte line, which every GPU that loads the library keeps until
+ * the process exits.  Hence nCells is limited to 16,777,216; larger sizes
+ * return CF_ERR_TOO_LARGE before anything is launched.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress): make
+ * it before any stream capture.  All calls on a device share the array, so
+ * calls whose kernels overlap on the GPU (different streams without
+ * ordering) race and give wrong dot products. */
+int cf_ldu_spmv_dot_noalloc(int32_t nCells, const float* diag,
+                            const float* upper, const float* lower,
+                            const int32_t* lowAddr, const int32_t* uppAddr,
+                            const int32_t* ownStartAddr,
+                            const int32_t* losortAddr,
+                            const int32_t* losortStartAddr, const float* x,
+                            const float* w, float* y, double* dot,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,8 @@ SIGNATURES = [
     ("cf_spmv32", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
     ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
     ("cf_time_kernel", C.c_int, [vp, i32, i32, C.POINTER(dbl)]),
+    ("cf_ldu_spmv_dot_noalloc", C.c_int, [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                          vp]),
 ]
 
 
