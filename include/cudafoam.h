@@ -213,6 +213,34 @@ int cf_solve_device(cf_context* ctx, int32_t solver, double* psi,
  * (metalFoamSolver.C:112-117,429-434). */
 int cf_residual(cf_context* ctx, int32_t which, double* r);
 
+/* ------------------------------------------------------------ adjoint */
+/* No counterpart in the reference (the design's differentiation row).
+ * For x = A^{-1} b and a loss L(x): lambda = A^{-T} dL/dx and
+ *   dL/db = lambda, dL/ddiag[i] = -lambda[i] x[i],
+ *   dL/dupper[f] = -lambda[l(f)] x[u(f)], dL/dlower[f] = -lambda[u(f)] x[l(f)]
+ * (upper[f] = A[l(f),u(f)], lower[f] = A[u(f),l(f)]).  A^T in LDU form is A
+ * with upper and lower exchanged: the transpose solve reuses the forward
+ * kernels on restaged values. */
+
+/* on != 0: stage A^T for the following solves/operators; 0: back to A. */
+int cf_set_transpose(cf_context* ctx, int32_t on);
+/* The gradient pass alone (face order / caller's cell order). */
+int cf_face_gradients(cf_context* ctx, const double* lambda, const double* x,
+                      double* dUpper, double* dLower, double* dDiag);
+int cf_face_gradients_device(cf_context* ctx, const double* lambda,
+                             const double* x, double* dUpper, double* dLower,
+                             double* dDiag);
+/* Adjoint solve (A^T lambda = dLdx from lambda0 = 0, same driver and
+ * options as cf_solve) followed by the gradient pass; leaves A staged. */
+int cf_solve_adjoint(cf_context* ctx, int32_t solver, const double* x,
+                     const double* dLdx, double* lambda, double* dUpper,
+                     double* dLower, double* dDiag, const cf_options* opts,
+                     cf_performance* perf);
+int cf_solve_adjoint_device(cf_context* ctx, int32_t solver, const double* x,
+                            const double* dLdx, double* lambda,
+                            double* dUpper, double* dLower, double* dDiag,
+                            const cf_options* opts, cf_performance* perf);
+
 /* ------------------------------------------------------------ operators */
 
 /* y = A x in FP64 with lduMatrix::Amul's per-row summation order

@@ -91,6 +91,13 @@ SIGNATURES = [
     ("cf_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_solve_device", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_residual", C.c_int, [vp, i32, vp]),
+    ("cf_set_transpose", C.c_int, [vp, i32]),
+    ("cf_face_gradients", C.c_int, [vp, vp, vp, vp, vp, vp]),
+    ("cf_face_gradients_device", C.c_int, [vp, vp, vp, vp, vp, vp]),
+    ("cf_solve_adjoint", C.c_int, [vp, i32, vp, vp, vp, vp, vp, vp, C.POINTER(Options),
+                                   C.POINTER(Performance)]),
+    ("cf_solve_adjoint_device", C.c_int, [vp, i32, vp, vp, vp, vp, vp, vp, C.POINTER(Options),
+                                          C.POINTER(Performance)]),
     ("cf_amul", C.c_int, [vp, vp, vp, i32]),
     ("cf_spmv32", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
     ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
@@ -243,6 +250,30 @@ class Context:
         check(load().cf_solve_device(self.h, int(solver), ptr(psi), ptr(source),
                                      C.byref(options), C.byref(perf)))
         return perf
+
+    def set_transpose(self, on=True):
+        check(load().cf_set_transpose(self.h, int(bool(on))))
+
+    def face_gradients(self, lam, x, nf):
+        lam = np.ascontiguousarray(lam, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        dU = np.empty(nf)
+        dL = np.empty(nf)
+        dD = np.empty_like(x)
+        check(load().cf_face_gradients(self.h, ptr(lam), ptr(x), ptr(dU), ptr(dL), ptr(dD)))
+        return dU, dL, dD
+
+    def solve_adjoint(self, solver, x, dLdx, nf, options):
+        x = np.ascontiguousarray(x, np.float64)
+        g = np.ascontiguousarray(dLdx, np.float64)
+        lam = np.empty_like(x)
+        dU = np.empty(nf)
+        dL = np.empty(nf)
+        dD = np.empty_like(x)
+        perf = Performance()
+        check(load().cf_solve_adjoint(self.h, int(solver), ptr(x), ptr(g), ptr(lam), ptr(dU),
+                                      ptr(dL), ptr(dD), C.byref(options), C.byref(perf)))
+        return lam, dU, dL, dD, perf
 
     def residual(self, n, which="final"):
         out = np.empty(n)

@@ -529,7 +529,11 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
     CF_TRY(dalloc(c, &c->d_io64, N));
     CF_TRY(dalloc(c, &c->d_io64b, N));
     CF_TRY(dalloc(c, &c->d_r0, N));
+    CF_TRY(dalloc(c, &c->d_gU, (size_t)std::max(nf, 1)));
+    CF_TRY(dalloc(c, &c->d_gL, (size_t)std::max(nf, 1)));
+    CF_TRY(dalloc(c, &c->d_gD, N));
     c->hasResidual = false;
+    c->transposed = false;
     CF_TRY(dalloc(c, &c->d_rA, N));
     CF_TRY(dalloc(c, &c->d_W0, N));
     CF_TRY(dalloc(c, &c->d_W1, N));
@@ -572,12 +576,25 @@ namespace cf {
 
 int stage_vals(cf_context* c, int sym32)
 {
+    // A^T in LDU form is A with upper and lower exchanged
+    const double* up = c->d_upper;
+    const double* lo = c->hasLower ? c->d_lower : c->d_upper;
+    if (c->transposed) std::swap(up, lo);
     const int g = grid_for(c, (const void*)k_stage_vals, c->nnzp);
-    k_stage_vals<<<g, NT, 0, c->stream>>>(c->nnzp, c->d_col, c->d_eface, c->d_upper,
-                                          c->hasLower ? c->d_lower : c->d_upper, sym32,
+    k_stage_vals<<<g, NT, 0, c->stream>>>(c->nnzp, c->d_col, c->d_eface, up, lo, sym32,
                                           c->d_val32, c->d_val64, c->d_valT64);
     CF_LAUNCH();
     c->val32Sym = sym32;
+    return CF_OK;
+}
+
+// u = A 1 (of the staged operator) and the deflation census
+int stage_rowsums(cf_context* c)
+{
+    auto fn = k_sumA<MAXW_UNROLL>;
+    const int g = grid_for(c, (const void*)fn, c->n);
+    fn<<<g, NT, 0, c->stream>>>(sell_of(c), c->d_diag64, c->d_u, c->d_drv, c->d_part);
+    CF_LAUNCH();
     return CF_OK;
 }
 
@@ -599,12 +616,7 @@ int stage_coeffs_from_device(cf_context* c)
         CF_LAUNCH();
     }
     CF_TRY(stage_vals(c, c->hasLower ? 0 : 1));
-    {
-        auto fn = k_sumA<MAXW_UNROLL>;
-        const int g = grid_for(c, (const void*)fn, c->n);
-        fn<<<g, NT, 0, c->stream>>>(sell_of(c), c->d_diag64, c->d_u, c->d_drv, c->d_part);
-        CF_LAUNCH();
-    }
+    CF_TRY(stage_rowsums(c));
     CF_TRY(stage_diag32(c, 0));
     c->hasCoeffs = true;
     return CF_OK;

@@ -70,6 +70,10 @@ struct cf_context
     double* d_io64b = nullptr;
     double* d_r0 = nullptr;                // residual at the entry of the last solve
     bool hasResidual = false;
+    bool transposed = false;               // operator staged as A^T (adjoint solves)
+    double* d_gU = nullptr;                // face gradients (face order)
+    double* d_gL = nullptr;
+    double* d_gD = nullptr;                // diagonal gradient (caller order)
     float* d_rA = nullptr;
     float* d_W0 = nullptr;
     float* d_W1 = nullptr;
@@ -108,5 +112,6 @@ PcgBufs pcg_bufs(const cf_context* c);
 BicgBufs bicg_bufs(const cf_context* c);
 int stage_vals(cf_context* c, int sym32);
 int stage_diag32(cf_context* c, int deflate);
+int stage_rowsums(cf_context* c);
 
 }  // namespace cf

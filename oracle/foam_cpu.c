@@ -360,7 +360,36 @@ int orc_cg64(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
     for (int32_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
     if (!lower)
     {
-        /* Jacobi-preconditioned conjugate gradients */
+        /* Deflated Jacobi-PCG (Nicolaides deflation with the constant vector,
+         * Z = 1): pressure matrices with one pinned cell have a weakly held
+         * constant mode, and right-hand sides with a large mean give
+         * solutions with a large constant offset that plain CG resolves
+         * slowly and only to offset-limited accuracy.  With u = A 1 and
+         * sigma = 1.u: P = I - u 1^T/sigma, CG on P A xt = P b, and
+         * x = 1 (1.b)/sigma + xt - 1 (u.xt)/sigma; the residual of x equals
+         * P (b - A xt), the quantity iterated on.  Starts from x = 0. */
+        double* u = (double*)malloc(nb);
+        double* xt = (double*)malloc(nb);
+        for (int32_t i = 0; i < n; ++i) z[i] = 1.0;
+        orc_amul_rows(n, low, upp, ownStart, losort, losortStart, diag, upper, NULL, z, u,
+                      transpose, nt);
+        double sigma = 0.0;
+        for (int32_t i = 0; i < n; ++i) sigma += u[i];
+        const int defl = sigma > 0.0;
+#define CF_PROJECT(v)                                          \
+    do                                                         \
+    {                                                          \
+        if (defl)                                              \
+        {                                                      \
+            double s_ = 0.0;                                   \
+            for (int32_t i = 0; i < n; ++i) s_ += (v)[i];      \
+            const double c_ = s_ / sigma;                      \
+            for (int32_t i = 0; i < n; ++i) (v)[i] -= c_ * u[i]; \
+        }                                                      \
+    } while (0)
+        memset(xt, 0, nb);
+        memcpy(r, b, nb);
+        CF_PROJECT(r);
         double rz = 0.0, rzold;
         for (it = 0; it < maxIter; ++it)
         {
@@ -376,20 +405,40 @@ int orc_cg64(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
             }
             orc_amul_rows(n, low, upp, ownStart, losort, losortStart, diag,
                           upper, NULL, p, q, transpose, nt);
+            CF_PROJECT(q);
             const double alpha = rz / sum_prod(n, p, q, nt);
             for (int32_t i = 0; i < n; ++i)
             {
-                x[i] += alpha * p[i];
+                xt[i] += alpha * p[i];
                 r[i] -= alpha * q[i];
             }
             if ((it + 1) % 50 == 0)
             {
-                /* recompute the true residual to stop FP64 drift */
+                /* recompute the true (deflated) residual to stop FP64 drift */
                 orc_amul_rows(n, low, upp, ownStart, losort, losortStart,
-                              diag, upper, NULL, x, q, transpose, nt);
+                              diag, upper, NULL, xt, q, transpose, nt);
                 for (int32_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+                CF_PROJECT(r);
             }
         }
+#undef CF_PROJECT
+        if (defl)
+        {
+            double sb = 0.0, ux = 0.0;
+            for (int32_t i = 0; i < n; ++i)
+            {
+                sb += b[i];
+                ux += u[i] * xt[i];
+            }
+            const double c = (sb - ux) / sigma;
+            for (int32_t i = 0; i < n; ++i) x[i] = xt[i] + c;
+        }
+        else
+        {
+            memcpy(x, xt, nb);
+        }
+        free(u);
+        free(xt);
     }
     else
     {
