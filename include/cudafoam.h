@@ -94,7 +94,9 @@ typedef struct
                                   CUDA-graph while loop, no host sync per
                                   iteration; 0: one host sync per batch of
                                   iterationsPerSync, as the reference      */
-    int32_t reserved;
+    int32_t stagnationLimit;   /* inner iterations without a new minimum of
+                                  sum|r| before the inner solve stops; 0
+                                  (default) = 50, metalFoamBackend.C:606   */
 } cf_options;
 
 /* solverPerformance plus the reference's profile/verbose figures
@@ -240,6 +242,44 @@ int cf_solve_adjoint_device(cf_context* ctx, int32_t solver, const double* x,
                             const double* dLdx, double* lambda,
                             double* dUpper, double* dLower, double* dDiag,
                             const cf_options* opts, cf_performance* perf);
+
+/* ------------------------------------------------------------ batches */
+/* No counterpart in the reference (the design's batching row).  A batch
+ * holds many independent symmetric pressure systems of any sizes and
+ * solves them together with cudaPCG semantics per system (same driver
+ * decisions, same stopping tests as cf_solve on each system alone): every
+ * phase of the iteration is one launch over all still-active systems and
+ * the iterations run in a device-side CUDA-graph loop until the last
+ * system has finished. */
+typedef struct cf_batch cf_batch;
+
+int cf_batch_create(cf_batch** out, int32_t device);
+int cf_batch_destroy(cf_batch* batch);
+int cf_batch_set_stream(cf_batch* batch, void* stream);
+int cf_batch_kernel_launches(const cf_batch* batch, long long* count);
+/* Adds one system (its lduAddressing, copied and validated); *index is its
+ * position.  All systems are added before cf_batch_finalize. */
+int cf_batch_add_system(cf_batch* batch, int32_t nCells, int32_t nFaces,
+                        const int32_t* lowAddr, const int32_t* uppAddr,
+                        const int32_t* ownStartAddr, const int32_t* losortAddr,
+                        const int32_t* losortStartAddr, int32_t* index);
+/* Lays all systems out on the device (reorder: CF_REORDER_*, per system). */
+int cf_batch_finalize(cf_batch* batch, int32_t reorder);
+/* FP64 coefficients of system `index` (lower must be NULL: symmetric). */
+int cf_batch_set_coeffs(cf_batch* batch, int32_t index, const double* diag,
+                        const double* upper, const double* lower);
+int cf_batch_set_coeffs_device(cf_batch* batch, int32_t index,
+                               const double* diag, const double* upper,
+                               const double* lower);
+/* Solves every system: psi[i] (in/out) and source[i] per system (host
+ * pointers; _device: device pointers), perf[i] per system.  solver must be
+ * CF_SOLVER_PCG. */
+int cf_batch_solve(cf_batch* batch, int32_t solver, double* const* psi,
+                   const double* const* source, const cf_options* opts,
+                   cf_performance* perf);
+int cf_batch_solve_device(cf_batch* batch, int32_t solver, double* const* psi,
+                          const double* const* source, const cf_options* opts,
+                          cf_performance* perf);
 
 /* ------------------------------------------------------------ operators */
 

@@ -45,7 +45,7 @@ class Options(C.Structure):
         ("minIter", C.c_int32), ("maxRestarts", C.c_int32), ("iterationsPerSync", C.c_int32),
         ("deflate", C.c_int32), ("chebyshevOrder", C.c_int32), ("chebyshevRatio", C.c_double),
         ("profile", C.c_int32), ("verbose", C.c_int32), ("graph", C.c_int32),
-        ("reserved", C.c_int32),
+        ("stagnationLimit", C.c_int32),
     ]
 
 
@@ -91,6 +91,18 @@ SIGNATURES = [
     ("cf_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_solve_device", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_residual", C.c_int, [vp, i32, vp]),
+    ("cf_batch_create", C.c_int, [C.POINTER(vp), i32]),
+    ("cf_batch_destroy", C.c_int, [vp]),
+    ("cf_batch_set_stream", C.c_int, [vp, vp]),
+    ("cf_batch_kernel_launches", C.c_int, [vp, C.POINTER(C.c_longlong)]),
+    ("cf_batch_add_system", C.c_int, [vp, i32, i32, vp, vp, vp, vp, vp, C.POINTER(i32)]),
+    ("cf_batch_finalize", C.c_int, [vp, i32]),
+    ("cf_batch_set_coeffs", C.c_int, [vp, i32, vp, vp, vp]),
+    ("cf_batch_set_coeffs_device", C.c_int, [vp, i32, vp, vp, vp]),
+    ("cf_batch_solve", C.c_int, [vp, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(Options),
+                                 C.POINTER(Performance)]),
+    ("cf_batch_solve_device", C.c_int, [vp, i32, C.POINTER(vp), C.POINTER(vp),
+                                        C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_set_transpose", C.c_int, [vp, i32]),
     ("cf_face_gradients", C.c_int, [vp, vp, vp, vp, vp, vp]),
     ("cf_face_gradients_device", C.c_int, [vp, vp, vp, vp, vp, vp]),
@@ -307,3 +319,67 @@ class Context:
         check(load().cf_cheb_apply(self.h, ptr(rr), ptr(z), int(order), float(beta),
                                    float(ratio)))
         return z
+
+
+class Batch:
+    """Many independent symmetric systems solved together (cf_batch_*)."""
+
+    def __init__(self, device: int = 0):
+        h = vp()
+        check(load().cf_batch_create(C.byref(h), int(device)))
+        self.h = h
+        self.sizes = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().cf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_system(self, addr):
+        arrs = [np.ascontiguousarray(a, np.int32) for a in addr.arrays()]
+        idx = C.c_int32()
+        check(load().cf_batch_add_system(self.h, int(addr.n), int(addr.nf),
+                                         *(ptr(a) for a in arrs), C.byref(idx)))
+        self.sizes.append((addr.n, addr.nf))
+        return idx.value
+
+    def finalize(self, reorder="auto"):
+        check(load().cf_batch_finalize(self.h, REORDER[reorder]))
+
+    def set_stream(self, stream_handle):
+        check(load().cf_batch_set_stream(self.h, vp(stream_handle) if stream_handle else None))
+
+    def kernel_launches(self):
+        n = C.c_longlong()
+        check(load().cf_batch_kernel_launches(self.h, C.byref(n)))
+        return n.value
+
+    def set_coeffs(self, i, diag, upper):
+        d = np.ascontiguousarray(diag, np.float64)
+        u = np.ascontiguousarray(upper, np.float64)
+        check(load().cf_batch_set_coeffs(self.h, int(i), ptr(d), ptr(u), None))
+
+    def set_coeffs_device(self, i, diag, upper):
+        check(load().cf_batch_set_coeffs_device(self.h, int(i), ptr(diag), ptr(upper), None))
+
+    def _solve(self, fn, psis, sources, options):
+        S = len(self.sizes)
+        pp = (vp * S)(*[ptr(p).value if ptr(p) is not None else None for p in psis])
+        ss = (vp * S)(*[ptr(s).value if ptr(s) is not None else None for s in sources])
+        perf = (Performance * S)()
+        check(fn(self.h, CF_SOLVER_PCG, pp, ss, C.byref(options), perf))
+        return list(perf)
+
+    def solve(self, psis, sources, options):
+        """psis: list of float64 arrays (updated in place), sources: list."""
+        srcs = [np.ascontiguousarray(s, np.float64) for s in sources]
+        return self._solve(load().cf_batch_solve, psis, srcs, options)
+
+    def solve_device(self, psis, sources, options):
+        return self._solve(load().cf_batch_solve_device, psis, sources, options)

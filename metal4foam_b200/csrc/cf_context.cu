@@ -217,6 +217,77 @@ void rcm_order(int32_t n, const int32_t* low, const int32_t* upp, const int32_t*
 
 namespace cf {
 
+int check_addressing(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
+                     const int32_t* own, const int32_t* los, const int32_t* losS)
+{
+    return validate_addressing(n, nf, low, upp, own, los, losS);
+}
+
+// Internal ordering + SELL-32 layout of one mesh on the host.
+int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
+                 const int32_t* own, const int32_t* los, const int32_t* losS, bool rcm,
+                 HostLayout& L)
+{
+    (void)nf;
+    std::vector<int32_t>& perm = L.perm;
+    perm.clear();
+    if (rcm) rcm_order(n, low, upp, own, los, losS, perm);
+    if ((int32_t)perm.size() != n)
+    {
+        perm.resize(n);
+        for (int32_t i = 0; i < n; ++i) perm[i] = i;
+    }
+    std::vector<int32_t> iperm(n);
+    for (int32_t r = 0; r < n; ++r) iperm[perm[r]] = r;
+
+    const int32_t nslices = (n + SLICE - 1) / SLICE;
+    L.sliceOff.assign(nslices + 1, 0);
+    long long nnzp = 0;
+    for (int32_t s = 0; s < nslices; ++s)
+    {
+        int32_t w = 0;
+        for (int32_t l = 0; l < SLICE; ++l)
+        {
+            const int32_t r = s * SLICE + l;
+            if (r >= n) break;
+            const int32_t i = perm[r];
+            w = std::max(w, (own[i + 1] - own[i]) + (losS[i + 1] - losS[i]));
+        }
+        nnzp += (long long)w * SLICE;
+        if (nnzp >= (1LL << 31) - 64)
+            return fail(CF_ERR_TOO_LARGE, "matrix too large for 32-bit entry offsets");
+        L.sliceOff[s + 1] = (int32_t)nnzp;
+    }
+    L.col.assign((size_t)std::max(nnzp, 1LL), -1);
+    L.eface.assign((size_t)std::max(nnzp, 1LL), -1);
+    int32_t maxw = 0;
+    for (int32_t r = 0; r < n; ++r)
+    {
+        const int32_t i = perm[r];
+        const int32_t s = r / SLICE;
+        const int32_t lane = r % SLICE;
+        int32_t k = 0;
+        for (int32_t f = own[i]; f < own[i + 1]; ++f, ++k)
+        {
+            const size_t e = (size_t)L.sliceOff[s] + (size_t)SLICE * k + lane;
+            L.col[e] = iperm[upp[f]];
+            L.eface[e] = f;
+        }
+        for (int32_t q = losS[i]; q < losS[i + 1]; ++q, ++k)
+        {
+            const int32_t f = los[q];
+            const size_t e = (size_t)L.sliceOff[s] + (size_t)SLICE * k + lane;
+            L.col[e] = (int32_t)((uint32_t)iperm[low[f]] | 0x80000000u);
+            L.eface[e] = f;
+        }
+        maxw = std::max(maxw, k);
+    }
+    L.nslices = nslices;
+    L.nnzp = nnzp;
+    L.maxw = maxw;
+    return CF_OK;
+}
+
 int grid_for(cf_context* c, const void* fn, long long work)
 {
     int occ = 0;
@@ -441,63 +512,17 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
     CF_CUDA(cudaStreamSynchronize(c->stream));
     free_topology(c);
 
-    // internal ordering
-    std::vector<int32_t> perm;
     const bool rcm = c->reorderMode == CF_REORDER_RCM ||
                      (c->reorderMode == CF_REORDER_AUTO && n > 65536);
-    if (rcm)
-        rcm_order(n, low, upp, own, los, losS, perm);
-    if ((int32_t)perm.size() != n)
-    {
-        perm.resize(n);
-        for (int32_t i = 0; i < n; ++i) perm[i] = i;
-    }
-    std::vector<int32_t> iperm(n);
-    for (int32_t r = 0; r < n; ++r) iperm[perm[r]] = r;
-
-    // SELL-32 layout
-    const int32_t nslices = (n + SLICE - 1) / SLICE;
-    std::vector<int32_t> sliceOff(nslices + 1, 0);
-    long long nnzp = 0;
-    for (int32_t s = 0; s < nslices; ++s)
-    {
-        int32_t w = 0;
-        for (int32_t l = 0; l < SLICE; ++l)
-        {
-            const int32_t r = s * SLICE + l;
-            if (r >= n) break;
-            const int32_t i = perm[r];
-            w = std::max(w, (own[i + 1] - own[i]) + (losS[i + 1] - losS[i]));
-        }
-        nnzp += (long long)w * SLICE;
-        if (nnzp >= (1LL << 31) - 64)
-            return fail(CF_ERR_TOO_LARGE, "matrix too large for 32-bit entry offsets");
-        sliceOff[s + 1] = (int32_t)nnzp;
-    }
-    std::vector<int32_t> col((size_t)std::max(nnzp, 1LL), -1);
-    std::vector<int32_t> eface((size_t)std::max(nnzp, 1LL), -1);
-    int32_t maxw = 0;
-    for (int32_t r = 0; r < n; ++r)
-    {
-        const int32_t i = perm[r];
-        const int32_t s = r / SLICE;
-        const int32_t lane = r % SLICE;
-        int32_t k = 0;
-        for (int32_t f = own[i]; f < own[i + 1]; ++f, ++k)
-        {
-            const size_t e = (size_t)sliceOff[s] + (size_t)SLICE * k + lane;
-            col[e] = iperm[upp[f]];
-            eface[e] = f;
-        }
-        for (int32_t q = losS[i]; q < losS[i + 1]; ++q, ++k)
-        {
-            const int32_t f = los[q];
-            const size_t e = (size_t)sliceOff[s] + (size_t)SLICE * k + lane;
-            col[e] = (int32_t)((uint32_t)iperm[low[f]] | 0x80000000u);
-            eface[e] = f;
-        }
-        maxw = std::max(maxw, k);
-    }
+    HostLayout L;
+    CF_TRY(build_layout(n, nf, low, upp, own, los, losS, rcm, L));
+    std::vector<int32_t>& perm = L.perm;
+    std::vector<int32_t>& sliceOff = L.sliceOff;
+    std::vector<int32_t>& col = L.col;
+    std::vector<int32_t>& eface = L.eface;
+    const int32_t nslices = L.nslices;
+    const long long nnzp = L.nnzp;
+    const int32_t maxw = L.maxw;
 
     c->n = n;
     c->nf = nf;

@@ -104,6 +104,24 @@ struct cf_context
 
 namespace cf {
 
+// Host-side SELL-32 layout of one mesh (see cf_internal.cuh).
+struct HostLayout
+{
+    std::vector<int32_t> perm;      // internal row -> caller's cell
+    std::vector<int32_t> sliceOff;  // nslices + 1
+    std::vector<int32_t> col;       // internal columns, bit 31 = neighbour side, -1 padding
+    std::vector<int32_t> eface;     // face of each entry, -1 padding
+    int32_t nslices = 0;
+    long long nnzp = 0;
+    int32_t maxw = 0;
+};
+
+int check_addressing(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
+                     const int32_t* own, const int32_t* los, const int32_t* losS);
+int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
+                 const int32_t* own, const int32_t* los, const int32_t* losS, bool rcm,
+                 HostLayout& L);
+
 int fail(int code, const std::string& msg);
 double wall_now();
 int grid_for(cf_context* c, const void* fn, long long work);

@@ -53,7 +53,7 @@ struct InnerState
     double wArA, wArAold, wApA, alpha, beta, res;
     double rA0rA, rA0rAold, rA0AyA, omega, tAtA, tAsA, resS;
     double bestRes, target, finalResSum;
-    int it, maxIter, ips, lastSync, noProgress;
+    int it, maxIter, ips, lastSync, noProgress, stagLimit;
     int cur, best, nxt;             // correction buffer indices (0..2)
     int converged, singular, stagnated, done, early;
     int sel;                        // buffer holding the returned correction

@@ -607,9 +607,11 @@ struct PcgBufs
     int n;
 };
 
-static __global__ void k_inner_setup(InnerState* st, double target, int maxIter, int ips)
+static __global__ void k_inner_setup(InnerState* st, double target, int maxIter, int ips,
+                                     int stagLimit = STAG_LIMIT)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    st->stagLimit = stagLimit > 0 ? stagLimit : STAG_LIMIT;
     st->wArA = st->wArAold = st->wApA = st->alpha = st->beta = st->res = 0.0;
     st->rA0rA = st->rA0rAold = st->rA0AyA = st->omega = st->tAtA = st->tAsA = st->resS = 0.0;
     st->bestRes = 1.0e300;
@@ -773,7 +775,7 @@ __device__ __forceinline__ void inner_sync_point(InnerState* st, bool checkWApA)
                 st->converged = 1;
                 st->done = 1;
             }
-            else if (st->noProgress >= STAG_LIMIT)
+            else if (st->noProgress >= st->stagLimit)
             {
                 st->stagnated = 1;
                 st->done = 1;

@@ -200,7 +200,7 @@ int get_graph(cf_context* c, int kind, int order, cudaGraphExec_t* out, int* bod
 // the right-hand side; `mean` (device, may be NULL) is subtracted from it.
 // kind 0: PCG (metalFoamBackend::pcg), 1: BiCGStab (::bicgstab).
 int inner_solve(cf_context* c, int kind, const double* mean, double target, int maxIter, int ips,
-                int order, int useGraph, cf_inner_stats* stats)
+                int order, int useGraph, cf_inner_stats* stats, int stagLimit = STAG_LIMIT)
 {
     const double tw0 = wall_now();
     cudaStream_t s = c->stream;
@@ -208,7 +208,7 @@ int inner_solve(cf_context* c, int kind, const double* mean, double target, int 
     {
         if (order > CF_MAX_CHEB) return fail(CF_ERR_INVALID_ARG, "chebyshevOrder too large");
     }
-    k_inner_setup<<<1, 32, 0, s>>>(c->d_st, target, maxIter, ips);
+    k_inner_setup<<<1, 32, 0, s>>>(c->d_st, target, maxIter, ips, stagLimit);
     CF_LAUNCH();
     const PcgBufs B = pcg_bufs(c);
     if (kind == 0)
@@ -415,7 +415,8 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
             }
             cf_inner_stats st;
             CF_TRY(inner_solve(c, bicg ? 1 : 0, meanp, target, o->maxIter - totalIter,
-                               o->iterationsPerSync, order, o->graph, &st));
+                               o->iterationsPerSync, order, o->graph, &st,
+                               o->stagnationLimit > 0 ? o->stagnationLimit : STAG_LIMIT));
             totalIter += st.nIterations;
             perf->tGpu += st.tGpuSeconds;
             perf->tInner += st.tWallSeconds;

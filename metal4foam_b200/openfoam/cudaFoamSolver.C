@@ -195,6 +195,7 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     opts.profile = cudaDict_.getOrDefault<bool>("profile", false);
     opts.verbose = cudaDict_.getOrDefault<bool>("verbose", false);
     opts.graph = cudaDict_.getOrDefault<bool>("graph", true);
+    opts.stagnationLimit = cudaDict_.getOrDefault<label>("stagnationLimit", 0);
 
     cf_performance perf;
     check

@@ -142,7 +142,7 @@ def backend_cache_clear():
 
 
 _CONTROL_KEYS = ("maxRestarts", "iterationsPerSync", "deflate", "chebyshevOrder",
-                 "chebyshevRatio", "profile", "verbose", "graph")
+                 "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit")
 
 
 class cudaFoamSolver:
@@ -199,6 +199,7 @@ class cudaFoamSolver:
             profile=bool(s.get("profile", False)),
             verbose=bool(s.get("verbose", False)),
             graph=bool(s.get("graph", True)),
+            stagnationLimit=int(s.get("stagnationLimit", 0)),
         )
 
     def solveImpl(self, psi: np.ndarray, source: np.ndarray, cmpt: int = 0) -> solverPerformance:
