@@ -217,6 +217,154 @@ def cpu_baseline(sysm, budget_s):
                        "cores": 1}}
 
 
+def time_cuda(fn, steps, stream):
+    """Device time (ms) of `steps` calls of fn, CUDA events on `stream`."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_batched(local, stream, steps=3):
+    """48 independent pressure systems (log-uniform 1e3..1e6 cells): one
+    batched solve vs the plain one-solve-at-a-time loop (graph-driven
+    single solves) and vs a host-synchronised plain loop (one host sync per
+    iteration, the reference's structure), all inputs resident, same
+    options; solves/s = 48 / time."""
+    import torch
+
+    from metal4foam_b200 import _lib, mesh
+    dev = torch.device("cuda", local)
+    systems = mesh.batched_systems()
+    opts = dict(stagnationLimit=400, maxRestarts=20, maxIter=20000)
+    dd = [torch.from_numpy(s.diag).to(dev) for s in systems]
+    du = [torch.from_numpy(s.upper).to(dev) for s in systems]
+    db = [torch.from_numpy(s.source).to(dev) for s in systems]
+    dp = [torch.zeros(s.n, dtype=torch.float64, device=dev) for s in systems]
+    bt = _lib.Batch(local)
+    bt.set_stream(stream.cuda_stream)
+    for s in systems:
+        bt.add_system(s.addr)
+    bt.finalize()
+    o = _lib.default_options(**opts)
+    res = {}
+
+    def batched():
+        for p in dp:
+            p.zero_()
+        for i in range(len(systems)):
+            bt.set_coeffs_device(i, dd[i], du[i])
+        res["b"] = bt.solve_device(dp, db, o)
+
+    batched()
+    ms_b = time_cuda(batched, steps, stream) / steps
+    ok_b = all(p.converged and p.finalResidual < 1e-6 for p in res["b"])
+    it_b = [p.nIterations for p in res["b"]]
+    ctxs = []
+    for s in systems:
+        c = _lib.Context(local)
+        c.set_stream(stream.cuda_stream)
+        a = s.addr
+        c.set_topology(a.n, a.nf, *a.arrays())
+        ctxs.append(c)
+
+    def plain(graph):
+        oo = _lib.default_options(graph=graph, **opts)
+
+        def run():
+            out = []
+            for i in range(len(systems)):
+                dp[i].zero_()
+                ctxs[i].set_coeffs_device(dd[i], du[i])
+                out.append(ctxs[i].solve_device(_lib.CF_SOLVER_PCG, dp[i], db[i], oo))
+            res["p"] = out
+        return run
+
+    plain(1)()
+    ms_p = time_cuda(plain(1), steps, stream) / steps
+    it_p = [p.nIterations for p in res["p"]]
+    ok_p = all(p.converged and p.finalResidual < 1e-6 for p in res["p"])
+    ms_h = time_cuda(plain(0), 1, stream)
+    for c in ctxs:
+        c.close()
+    bt.close()
+    S = len(systems)
+    return {"workload": f"{S} independent varcoeff pressure systems, 2-D/3-D, "
+                        f"{sum(s.n for s in systems)} cells (log-uniform 1e3..1e6 per system)",
+            "options": opts, "all_converged_1e-6": bool(ok_b and ok_p),
+            "iterations_identical_to_plain": it_b == it_p,
+            "batched_solves_per_s": round(S / (ms_b / 1e3), 2),
+            "plain_loop_solves_per_s": round(S / (ms_p / 1e3), 2),
+            "host_sync_loop_solves_per_s": round(S / (ms_h / 1e3), 2),
+            "speedup_vs_plain_loop": round(ms_p / ms_b, 3),
+            "speedup_vs_host_sync_loop": round(ms_h / ms_b, 3),
+            "ms": {"batched": round(ms_b, 2), "plain": round(ms_p, 2),
+                   "host_sync": round(ms_h, 2)}}
+
+
+def run_adjoint(local, stream, steps=3):
+    """64^3 variable-coefficient Poisson, L = 0.5||x - x*||^2: forward solve
+    to FP64 1e-10 vs the adjoint (transpose solve to 1e-9 + face-gradient
+    pass), inputs resident."""
+    import torch
+
+    from metal4foam_b200 import _lib, mesh
+    dev = torch.device("cuda", local)
+    s, xstar = mesh.adjoint_system((64, 64, 64), seed=5)
+    ctx = _lib.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    d_diag = torch.from_numpy(s.diag).to(dev)
+    d_up = torch.from_numpy(s.upper).to(dev)
+    d_b = torch.from_numpy(s.source).to(dev)
+    d_xs = torch.from_numpy(xstar).to(dev)
+    x = torch.zeros(s.n, dtype=torch.float64, device=dev)
+    g = torch.zeros_like(x)
+    lam = torch.zeros_like(x)
+    dU = torch.zeros(s.nf, dtype=torch.float64, device=dev)
+    dL = torch.zeros_like(dU)
+    dD = torch.zeros_like(x)
+    of = _lib.default_options(tolerance=1e-10, maxRestarts=12, maxIter=5000)
+    oa = _lib.default_options(tolerance=1e-9, maxRestarts=12, maxIter=5000)
+    L = _lib.load()
+    perf = {}
+
+    def forward():
+        x.zero_()
+        ctx.set_coeffs_device(d_diag, d_up, None)
+        perf["f"] = ctx.solve_device(_lib.CF_SOLVER_PCG, x, d_b, of)
+
+    def adjoint():
+        torch.sub(x, d_xs, out=g)
+        p = _lib.Performance()
+        _lib.check(L.cf_solve_adjoint_device(ctx.h, _lib.CF_SOLVER_PCG, _lib.ptr(x), _lib.ptr(g),
+                                             _lib.ptr(lam), _lib.ptr(dU), _lib.ptr(dL),
+                                             _lib.ptr(dD), _lib.C.byref(oa), _lib.C.byref(p)))
+        perf["a"] = p
+
+    forward()
+    adjoint()
+    ms_f = time_cuda(forward, steps, stream) / steps
+    ms_a = time_cuda(adjoint, steps, stream) / steps
+    ctx.close()
+    return {"workload": "varcoeff Poisson 64^3 (262,144 cells), L = 0.5||x - x*||^2",
+            "forward_ms": round(ms_f, 3), "adjoint_ms": round(ms_a, 3),
+            "adjoint_over_forward": round(ms_a / ms_f, 3),
+            "gradient_total_over_forward": round((ms_f + ms_a) / ms_f, 3),
+            "forward_final_residual": perf["f"].finalResidual,
+            "adjoint_final_residual": perf["a"].finalResidual,
+            "forward_iterations": perf["f"].nIterations,
+            "adjoint_iterations": perf["a"].nIterations,
+            "converged": bool(perf["f"].converged and perf["a"].converged)}
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -348,6 +496,9 @@ def run_ours(args, ws, rank, local):
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
+        if not args.no_extras:
+            out["batched"] = run_batched(local, stream)
+            out["adjoint"] = run_adjoint(local, stream)
         if ws == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(sysm, args.cpu_budget)
     ctx.close()
@@ -401,6 +552,8 @@ def main():
     ap.add_argument("--ref-step-seconds", type=float, default=5.0,
                     help="CPU seconds per step of --impl reference")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and adjoint measurements")
     ap.add_argument("--graph", type=int, default=1,
                     help="1: inner iterations in a CUDA-graph while loop (default); 0: one "
                          "host sync per iteration (same kernels; ncu cannot profile kernels "
