@@ -281,6 +281,25 @@ int cf_batch_solve_device(cf_batch* batch, int32_t solver, double* const* psi,
                           const double* const* source, const cf_options* opts,
                           cf_performance* perf);
 
+/* ------------------------------------------------------------ several RHS */
+/* No counterpart in the reference (the design's multi-RHS row): the
+ * reference solves the components of a vector equation one after another
+ * (fvMatrix<vector>::solveSegregated calls the scalar solver per
+ * component).  cf_solve_multi solves nrhs systems A psi_k = source_k on the
+ * matrix of the last cf_set_coeffs together: psi and source hold nrhs
+ * component fields of nCells each (component k at offset k*nCells), perf
+ * has nrhs entries.  Every SpMV reads the matrix once for up to 4
+ * components; each component keeps its own scalars, early exit, stopping
+ * tests and restarts, and its results equal those of cf_solve on that
+ * component alone.  solver must be CF_SOLVER_PBICGSTAB (momentum).
+ * cf_residual keeps referring to the last single solve. */
+int cf_solve_multi(cf_context* ctx, int32_t solver, int32_t nrhs, double* psi,
+                   const double* source, const cf_options* opts,
+                   cf_performance* perf);
+int cf_solve_multi_device(cf_context* ctx, int32_t solver, int32_t nrhs,
+                          double* psi, const double* source,
+                          const cf_options* opts, cf_performance* perf);
+
 /* ------------------------------------------------------------ operators */
 
 /* y = A x in FP64 with lduMatrix::Amul's per-row summation order

@@ -91,6 +91,10 @@ SIGNATURES = [
     ("cf_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_solve_device", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_residual", C.c_int, [vp, i32, vp]),
+    ("cf_solve_multi", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
+                                 C.POINTER(Performance)]),
+    ("cf_solve_multi_device", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
+                                        C.POINTER(Performance)]),
     ("cf_batch_create", C.c_int, [C.POINTER(vp), i32]),
     ("cf_batch_destroy", C.c_int, [vp]),
     ("cf_batch_set_stream", C.c_int, [vp, vp]),
@@ -262,6 +266,24 @@ class Context:
         check(load().cf_solve_device(self.h, int(solver), ptr(psi), ptr(source),
                                      C.byref(options), C.byref(perf)))
         return perf
+
+    def solve_multi(self, solver, psi, source, options):
+        """psi, source: C-contiguous float64 (nrhs, nCells); psi in place."""
+        nrhs = int(psi.shape[0])
+        if source.shape != psi.shape:
+            raise ValueError("psi and source shapes differ")
+        perf = (Performance * nrhs)()
+        check(load().cf_solve_multi(self.h, int(solver), nrhs, ptr(psi), ptr(source),
+                                    C.byref(options), perf))
+        return list(perf)
+
+    def solve_multi_device(self, solver, psi, source, options):
+        """psi, source: device tensors (nrhs, nCells) float64."""
+        nrhs = int(psi.shape[0])
+        perf = (Performance * nrhs)()
+        check(load().cf_solve_multi_device(self.h, int(solver), nrhs, ptr(psi), ptr(source),
+                                           C.byref(options), perf))
+        return list(perf)
 
     def set_transpose(self, on=True):
         check(load().cf_set_transpose(self.h, int(bool(on))))

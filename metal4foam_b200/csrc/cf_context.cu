@@ -83,6 +83,7 @@ int dalloc(cf_context* c, T** p, size_t count)
 
 void free_topology(cf_context* c)
 {
+    cf_multi_release(c);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();
     for (void* p : c->topoAllocs) cudaFree(p);

@@ -100,7 +100,13 @@ struct cf_context
 
     // instantiated inner-loop graphs keyed by (kind, chebyshev order)
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+
+    // several right-hand sides on this matrix (cf_multi.cu), built on first use
+    void* multi = nullptr;
 };
+
+// Frees the multi-RHS buffers and graphs (with the topology they point into).
+void cf_multi_release(cf_context* c);
 
 namespace cf {
 
