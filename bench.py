@@ -16,7 +16,10 @@ the coefficients, psi and source inside the timed region.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 runs one independent replica per GPU (torchrun; the single system is
-not partitioned), value = all replicas' solves / max-over-ranks time.
+not partitioned), value = all replicas' solves / max-over-ranks time.  The
+batched extra (48 independent systems) is sharded: each rank solves its
+share of the systems, assigned by SpMV-byte bin packing, and only the
+statuses travel (gathered to rank 0).
 ``--impl reference`` times the reference's CPU path (OpenFOAM's FP64 PCG,
 restated in oracle/) on the host cores instead.
 """
@@ -231,43 +234,55 @@ def time_cuda(fn, steps, stream):
     return e0.elapsed_time(e1)
 
 
-def run_batched(local, stream, steps=3):
+def run_batched(local, stream, ws=1, rank=0, steps=3):
     """48 independent pressure systems (log-uniform 1e3..1e6 cells): one
     batched solve vs the plain one-solve-at-a-time loop (graph-driven
     single solves) and vs a host-synchronised plain loop (one host sync per
     iteration, the reference's structure), all inputs resident, same
-    options; solves/s = 48 / time."""
+    options; solves/s = 48 / time.  With N ranks the systems are shared out
+    by SpMV-byte bin packing (metal4foam_b200.shard), each rank solves its
+    share, times are the max over ranks and the statuses are gathered to
+    rank 0 (the only exchange).  Collective on every rank when N > 1."""
     import torch
 
-    from metal4foam_b200 import _lib, mesh
+    from metal4foam_b200 import _lib, mesh, shard
     dev = torch.device("cuda", local)
     systems = mesh.batched_systems()
+    S = len(systems)
+    mine = shard.partition([shard.spmv_bytes(s.n, s.nf) for s in systems], ws)[rank]
+    loc = [systems[i] for i in mine]
     opts = dict(stagnationLimit=400, maxRestarts=20, maxIter=20000)
-    dd = [torch.from_numpy(s.diag).to(dev) for s in systems]
-    du = [torch.from_numpy(s.upper).to(dev) for s in systems]
-    db = [torch.from_numpy(s.source).to(dev) for s in systems]
-    dp = [torch.zeros(s.n, dtype=torch.float64, device=dev) for s in systems]
-    bt = _lib.Batch(local)
-    bt.set_stream(stream.cuda_stream)
-    for s in systems:
-        bt.add_system(s.addr)
-    bt.finalize()
+    dd = [torch.from_numpy(s.diag).to(dev) for s in loc]
+    du = [torch.from_numpy(s.upper).to(dev) for s in loc]
+    db = [torch.from_numpy(s.source).to(dev) for s in loc]
+    dp = [torch.zeros(s.n, dtype=torch.float64, device=dev) for s in loc]
+    bt = None
+    if loc:
+        bt = _lib.Batch(local)
+        bt.set_stream(stream.cuda_stream)
+        for s in loc:
+            bt.add_system(s.addr)
+        bt.finalize()
     o = _lib.default_options(**opts)
-    res = {}
+    res = {"b": [], "p": []}
 
     def batched():
+        if bt is None:
+            return
         for p in dp:
             p.zero_()
-        for i in range(len(systems)):
+        for i in range(len(loc)):
             bt.set_coeffs_device(i, dd[i], du[i])
         res["b"] = bt.solve_device(dp, db, o)
 
+    def timed(fn, k):
+        barrier(ws)
+        return max_over_ranks(time_cuda(fn, k, stream), ws)
+
     batched()
-    ms_b = time_cuda(batched, steps, stream) / steps
-    ok_b = all(p.converged and p.finalResidual < 1e-6 for p in res["b"])
-    it_b = [p.nIterations for p in res["b"]]
+    ms_b = timed(batched, steps) / steps
     ctxs = []
-    for s in systems:
+    for s in loc:
         c = _lib.Context(local)
         c.set_stream(stream.cuda_stream)
         a = s.addr
@@ -279,7 +294,7 @@ def run_batched(local, stream, steps=3):
 
         def run():
             out = []
-            for i in range(len(systems)):
+            for i in range(len(loc)):
                 dp[i].zero_()
                 ctxs[i].set_coeffs_device(dd[i], du[i])
                 out.append(ctxs[i].solve_device(_lib.CF_SOLVER_PCG, dp[i], db[i], oo))
@@ -287,18 +302,28 @@ def run_batched(local, stream, steps=3):
         return run
 
     plain(1)()
-    ms_p = time_cuda(plain(1), steps, stream) / steps
+    ms_p = timed(plain(1), steps) / steps
     it_p = [p.nIterations for p in res["p"]]
     ok_p = all(p.converged and p.finalResidual < 1e-6 for p in res["p"])
-    ms_h = time_cuda(plain(0), 1, stream)
+    ms_h = timed(plain(0), 1)
     for c in ctxs:
         c.close()
-    bt.close()
-    S = len(systems)
+    if bt is not None:
+        bt.close()
+    recs = shard.gather_records(mine, [shard.perf_record(p) for p in res["b"]], S, rank, ws)
+    same = shard.gather_records(mine, [{"same": int(p.nIterations == q)} for p, q in
+                                       zip(res["b"], it_p)], S, rank, ws)
+    okp = shard.gather_records(mine, [{"ok": int(ok_p)} for _ in mine], S, rank, ws)
+    if rank != 0:
+        return None
+    ok_b = all(r["converged"] and r["finalResidual"] < 1e-6 for r in recs)
     return {"workload": f"{S} independent varcoeff pressure systems, 2-D/3-D, "
                         f"{sum(s.n for s in systems)} cells (log-uniform 1e3..1e6 per system)",
-            "options": opts, "all_converged_1e-6": bool(ok_b and ok_p),
-            "iterations_identical_to_plain": it_b == it_p,
+            "options": opts, "ranks": ws,
+            "sharding": "one batch per rank, systems by SpMV-byte bin packing; statuses "
+                        "gathered to rank 0" if ws > 1 else "one batch",
+            "all_converged_1e-6": bool(ok_b and all(r["ok"] for r in okp)),
+            "iterations_identical_to_plain": all(r["same"] for r in same),
             "batched_solves_per_s": round(S / (ms_b / 1e3), 2),
             "plain_loop_solves_per_s": round(S / (ms_p / 1e3), 2),
             "host_sync_loop_solves_per_s": round(S / (ms_h / 1e3), 2),
@@ -512,6 +537,9 @@ def run_ours(args, ws, rank, local):
     e2e_ok = all(p.converged and p.finalResidual < 1e-6 for p in e2e_perfs)
     backend_cache_clear()
 
+    batched = None
+    if not args.no_extras:
+        batched = run_batched(local, stream, ws, rank)   # collective when N > 1
     out = None
     if rank == 0:
         value = ws * args.steps / (ms_max / 1000.0)
@@ -547,7 +575,7 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": launches,
         }
         if not args.no_extras:
-            out["batched"] = run_batched(local, stream)
+            out["batched"] = batched
             out["adjoint"] = run_adjoint(local, stream)
             out["multi_rhs"] = run_multi_rhs(local, stream)
         if ws == 1 and not args.no_cpu:
