@@ -335,6 +335,59 @@ enum
 int cf_time_kernel(cf_context* ctx, int32_t which, int32_t reps,
                    double* msPerLaunch);
 
+/* ------------------------------------------------------------ autotuning */
+/* No counterpart in the reference (the design's autotuner row).  The SpMV
+ * inside the FP32 Krylov kernels (Chebyshev steps, p-update SpMV, both
+ * BiCGStab SpMVs, cf_spmv32, cf_cheb_apply) runs in one of several launch
+ * shapes:
+ *   layout CF_LAYOUT_SELL32: the SELL-32 copy of the matrix, one row per
+ *     thread (rowsPerWarp 32);
+ *   layout CF_LAYOUT_LDU: the reference's own addressing read directly
+ *     (ownerStartAddr ranges of upperAddr / upper, then losortStartAddr
+ *     ranges of losortAddr -> lowerAddr / lower, metalFoamKernels.metal:64-109),
+ *     rowsPerWarp 32 (row per thread), 8, 4 or 1 (warp per row: the lanes
+ *     of a row load its entries and form the products together);
+ *   blockSize 128, 256 or 512 threads; rhsTile 1..4 components per pass of
+ *   cf_solve_multi.
+ * Every shape forms each row of A x with the same operations in the same
+ * order (the products of a row are added one by one in the reference's
+ * entry order), so A x is bit-identical across shapes; dot products fold
+ * their partial sums in a shape-dependent order.  The default is SELL32,
+ * 32 rows per warp, 256 threads, rhsTile 4.  The batched kernels
+ * (cf_batch_*) and the multi-RHS kernels always use the default shape. */
+enum
+{
+    CF_LAYOUT_SELL32 = 0,
+    CF_LAYOUT_LDU = 1
+};
+
+typedef struct cf_spmv_config
+{
+    int32_t layout;
+    int32_t rowsPerWarp;
+    int32_t blockSize;
+    int32_t rhsTile;
+} cf_spmv_config;
+
+typedef struct cf_tune_entry
+{
+    cf_spmv_config config;
+    double msPerLaunch;     /* FP32 SpMV + dot, CUDA events, inputs in HBM  */
+} cf_tune_entry;
+
+int cf_spmv_config_default(cf_spmv_config* cfg);
+int cf_get_spmv_config(cf_context* ctx, cf_spmv_config* cfg);
+/* Validates and applies; CF_ERR_UNSUPPORTED for a shape not in the list. */
+int cf_set_spmv_config(cf_context* ctx, const cf_spmv_config* cfg);
+/* Times the FP32 SpMV in every shape on the context's matrix (reps launches
+ * each after one warm-up) and the multi-RHS SpMV for 1..4 components, then
+ * writes the fastest shape (and the RHS tile with the least time per
+ * component) to *best; apply != 0 also makes it the context's shape.
+ * table (capacity entries, may be NULL) receives every timing; *count the
+ * number of shapes timed. */
+int cf_autotune(cf_context* ctx, int32_t reps, int32_t apply, cf_spmv_config* best,
+                cf_tune_entry* table, int32_t capacity, int32_t* count);
+
 /* ------------------------------------------------------------ no allocation */
 
 /* y = A x and *dot = sum w.y for callers that cannot allocate device memory:

@@ -71,6 +71,30 @@ i32 = C.c_int32
 dbl = C.c_double
 
 # (name, restype, argtypes) of every exported function
+class SpmvConfig(C.Structure):
+    _fields_ = [("layout", C.c_int32), ("rowsPerWarp", C.c_int32), ("blockSize", C.c_int32),
+                ("rhsTile", C.c_int32)]
+
+    def as_dict(self):
+        return {"layout": LAYOUT_NAMES[self.layout], "rowsPerWarp": self.rowsPerWarp,
+                "blockSize": self.blockSize, "rhsTile": self.rhsTile}
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("config", SpmvConfig), ("msPerLaunch", C.c_double)]
+
+
+CF_LAYOUT_SELL32 = 0
+CF_LAYOUT_LDU = 1
+LAYOUTS = {"sell32": CF_LAYOUT_SELL32, "ldu": CF_LAYOUT_LDU}
+LAYOUT_NAMES = {v: k for k, v in LAYOUTS.items()}
+
+
+def spmv_config(layout="sell32", rowsPerWarp=32, blockSize=256, rhsTile=4):
+    return SpmvConfig(LAYOUTS[layout] if isinstance(layout, str) else int(layout),
+                      int(rowsPerWarp), int(blockSize), int(rhsTile))
+
+
 SIGNATURES = [
     ("cf_abi_version", C.c_int, []),
     ("cf_last_error", C.c_char_p, []),
@@ -91,6 +115,11 @@ SIGNATURES = [
     ("cf_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_solve_device", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Performance)]),
     ("cf_residual", C.c_int, [vp, i32, vp]),
+    ("cf_spmv_config_default", C.c_int, [C.POINTER(SpmvConfig)]),
+    ("cf_get_spmv_config", C.c_int, [vp, C.POINTER(SpmvConfig)]),
+    ("cf_set_spmv_config", C.c_int, [vp, C.POINTER(SpmvConfig)]),
+    ("cf_autotune", C.c_int, [vp, i32, i32, C.POINTER(SpmvConfig), C.POINTER(TuneEntry), i32,
+                              C.POINTER(i32)]),
     ("cf_solve_multi", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
                                  C.POINTER(Performance)]),
     ("cf_solve_multi_device", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
@@ -334,6 +363,28 @@ class Context:
         ms = C.c_double()
         check(load().cf_time_kernel(self.h, self.KERNELS[which], int(reps), C.byref(ms)))
         return ms.value
+
+    def spmv_config(self):
+        k = SpmvConfig()
+        check(load().cf_get_spmv_config(self.h, C.byref(k)))
+        return k
+
+    def set_spmv_config(self, cfg=None, **kw):
+        """Launch shape of the FP32 SpMV kernels: pass a SpmvConfig, or
+        keywords of :func:`spmv_config` (unnamed ones keep their defaults)."""
+        k = cfg if cfg is not None else spmv_config(**kw)
+        check(load().cf_set_spmv_config(self.h, C.byref(k)))
+
+    def autotune(self, reps=20, apply=True):
+        """Times every SpMV launch shape on this matrix; returns (best
+        config, [(config dict, ms per launch), ...])."""
+        best = SpmvConfig()
+        table = (TuneEntry * 64)()
+        count = C.c_int32()
+        check(load().cf_autotune(self.h, int(reps), int(bool(apply)), C.byref(best), table, 64,
+                                 C.byref(count)))
+        return best, [(table[i].config.as_dict(), table[i].msPerLaunch)
+                      for i in range(min(count.value, 64))]
 
     def cheb_apply(self, r, order, beta, ratio=30.0):
         rr = np.ascontiguousarray(r, np.float32)

@@ -88,6 +88,9 @@ void free_topology(cf_context* c)
     c->graphs.clear();
     for (void* p : c->topoAllocs) cudaFree(p);
     c->topoAllocs.clear();
+    c->lduReady = false;
+    c->d_own = c->d_losS = c->d_los = c->d_uppI = c->d_lowI = nullptr;
+    c->d_face32 = nullptr;
     c->hasTopo = false;
     c->hasCoeffs = false;
     c->n = c->nf = 0;
@@ -406,6 +409,7 @@ extern "C" int cf_context_create(cf_context** out, int32_t device)
     c->device = device;
     c->numSMs = prop.multiProcessorCount;
     c->maxBlocksPerSM = std::max(1, prop.maxThreadsPerMultiProcessor / NT);
+    c->maxCtasPerSM = std::max(c->maxBlocksPerSM, prop.maxBlocksPerMultiProcessor);
     c->l2Bytes = prop.l2CacheSize;
     cudaError_t e = cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking);
     if (e != cudaSuccess)
@@ -414,7 +418,9 @@ extern "C" int cf_context_create(cf_context** out, int32_t device)
         return fail(CF_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
     c->stream = c->ownStream;
-    const size_t partCount = (size_t)NPART * c->numSMs * c->maxBlocksPerSM;
+    // reduction partials: NPART values for every block any launch shape can
+    // keep resident (variant grids of 128-thread blocks exceed maxBlocksPerSM)
+    const size_t partCount = (size_t)NPART * c->numSMs * c->maxCtasPerSM;
     if (cudaMalloc((void**)&c->d_part, partCount * sizeof(double)) != cudaSuccess ||
         cudaMalloc((void**)&c->d_st, sizeof(InnerState)) != cudaSuccess ||
         cudaMalloc((void**)&c->d_drv, sizeof(DriverState)) != cudaSuccess ||
@@ -611,6 +617,7 @@ int stage_vals(cf_context* c, int sym32)
                                           c->d_val32, c->d_val64, c->d_valT64);
     CF_LAUNCH();
     c->val32Sym = sym32;
+    if (c->lduReady) CF_TRY(stage_face32(c, up, lo, sym32));
     return CF_OK;
 }
 

@@ -103,6 +103,23 @@ struct cf_context
 
     // several right-hand sides on this matrix (cf_multi.cu), built on first use
     void* multi = nullptr;
+
+    // SpMV launch shape of the FP32 Krylov kernels (cf_tune.cu): layout
+    // (CF_LAYOUT_*), rows per warp, block size, multi-RHS tile
+    int maxCtasPerSM = 32;
+    int cfgLayout = 0;
+    int cfgRowsPerWarp = 32;
+    int cfgBlockSize = 256;
+    int cfgRhsTile = 4;
+    // the reference's addressing read directly (CF_LAYOUT_LDU), built on
+    // first use; topology-lifetime allocations
+    bool lduReady = false;
+    int* d_own = nullptr;       // ownerStartAddr [n+1], caller's numbering
+    int* d_losS = nullptr;      // losortStartAddr [n+1]
+    int* d_los = nullptr;       // losortAddr [nf]
+    int* d_uppI = nullptr;      // internal row of upperAddr[f]
+    int* d_lowI = nullptr;      // internal row of lowerAddr[f]
+    float* d_face32 = nullptr;  // [2 nf]: FP32 upper, then FP32 lower (face order)
 };
 
 // Frees the multi-RHS buffers and graphs (with the topology they point into).
@@ -137,5 +154,21 @@ BicgBufs bicg_bufs(const cf_context* c);
 int stage_vals(cf_context* c, int sym32);
 int stage_diag32(cf_context* c, int deflate);
 int stage_rowsums(cf_context* c);
+
+// Launch-shape variants of the SpMV-carrying FP32 kernels (cf_tune.cu).
+// spmv_default(c): the context runs the SELL-32 row-per-thread kernels of
+// cf_kernels.cuh with 256-thread blocks; otherwise the launches below run
+// the variant the configuration names.  Every variant forms each row of
+// A x with the same operations in the same order, so A x is bit-identical;
+// only the order in which the dot products are folded differs.
+bool spmv_default(const cf_context* c);
+int stage_face32(cf_context* c, const double* up, const double* lo, int sym32);
+int launch_cheb_step_v(cf_context* c, bool last, const PcgBufs& B, const float* zin,
+                       const float* win, float* wout, float* zout, int j);
+int launch_pcg_p_spmv_v(cf_context* c, const PcgBufs& B, const float* wA);
+int launch_bicg_b_v(cf_context* c, const BicgBufs& B);
+int launch_bicg_d_v(cf_context* c, const BicgBufs& B);
+int launch_spmv32_v(cf_context* c, const float* diag, const float* x, const float* w, float* y,
+                    double* out);
 
 }  // namespace cf

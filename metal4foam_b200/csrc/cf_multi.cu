@@ -989,9 +989,11 @@ int solve_multi(cf_context* c, int32_t solver, int32_t nrhs, double* psi, const 
     CF_CUDA(cudaSetDevice(c->device));
     if (c->transposed) return fail(CF_ERR_UNSUPPORTED, "transposed operator staged");
     const size_t n = (size_t)c->n;
-    for (int first = 0; first < nrhs; first += RMAX)
+    // components per pass: the context's RHS tile (cf_set_spmv_config / cf_autotune)
+    const int tile = std::max(1, std::min(RMAX, c->cfgRhsTile));
+    for (int first = 0; first < nrhs; first += tile)
     {
-        const int R = std::min(RMAX, nrhs - first);
+        const int R = std::min(tile, nrhs - first);
         double* p = psi + first * n;
         const double* b = src + first * n;
         cf_performance* pf = perf + first;

@@ -59,6 +59,12 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
             const float* zin = (j == 1) ? B.W0 : Z[chebz(j - 1)];
             const float* win = (j == 1) ? B.W0 : B.W1;
             float* zout = Z[chebz(j)];
+            if (!spmv_default(c))
+            {
+                CF_TRY(launch_cheb_step_v(c, j == order - 1, B, zin, win, B.W1, zout, j));
+                ++nk;
+                continue;
+            }
             if (j == order - 1)
             {
                 auto fn = k_cheb_step<true, MW>;
@@ -76,6 +82,12 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
         }
         wA = Z[chebz(order - 1)];
     }
+    if (!spmv_default(c))
+    {
+        CF_TRY(launch_pcg_p_spmv_v(c, B, wA));
+        ++nk;
+    }
+    else
     {
         auto fn = k_pcg_p_spmv<MW>;
         fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, wA, c->d_st, c->d_part);
@@ -105,6 +117,11 @@ int launch_bicg_body(cf_context* c, cudaGraphConditionalHandle h, int useCond, i
     cudaStream_t s = c->stream;
     k_bicg_a<<<grid_for(c, (const void*)k_bicg_a, c->n), NT, 0, s>>>(B, c->d_st);
     CF_LAUNCH();
+    if (!spmv_default(c))
+    {
+        CF_TRY(launch_bicg_b_v(c, B));
+    }
+    else
     {
         auto fn = k_bicg_b<MW>;
         fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
@@ -113,6 +130,11 @@ int launch_bicg_body(cf_context* c, cudaGraphConditionalHandle h, int useCond, i
     k_bicg_c<<<grid_for(c, (const void*)k_bicg_c, c->n), NT, 0, s>>>(B, c->d_st, c->d_part, h,
                                                                     useCond);
     CF_LAUNCH();
+    if (!spmv_default(c))
+    {
+        CF_TRY(launch_bicg_d_v(c, B));
+    }
+    else
     {
         auto fn = k_bicg_d<MW>;
         fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
@@ -643,12 +665,20 @@ extern "C" int cf_spmv32(cf_context* c, const float* x, const float* w, float* y
         k_gather_f32<<<g, NT, 0, s>>>(n, c->d_perm, c->d_io32, c->d_Z1);
         CF_LAUNCH();
     }
-    auto fn = k_spmv32<MW>;
-    fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(sell_of(c), c->d_diag32, c->d_Z0,
-                                                     w ? c->d_Z1 : nullptr, c->d_W1,
-                                                     c->d_scratch64, &c->d_drv->ticket,
-                                                     c->d_part);
-    CF_LAUNCH();
+    if (!spmv_default(c))
+    {
+        CF_TRY(launch_spmv32_v(c, c->d_diag32, c->d_Z0, w ? c->d_Z1 : nullptr, c->d_W1,
+                               c->d_scratch64));
+    }
+    else
+    {
+        auto fn = k_spmv32<MW>;
+        fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(sell_of(c), c->d_diag32, c->d_Z0,
+                                                         w ? c->d_Z1 : nullptr, c->d_W1,
+                                                         c->d_scratch64, &c->d_drv->ticket,
+                                                         c->d_part);
+        CF_LAUNCH();
+    }
     k_scatter_f32<<<g, NT, 0, s>>>(n, c->d_perm, c->d_W1, c->d_io32);
     CF_LAUNCH();
     CF_CUDA(cudaMemcpyAsync(y, c->d_io32, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
@@ -688,10 +718,17 @@ extern "C" int cf_cheb_apply(cf_context* c, const float* r, float* z, int32_t or
     {
         const float* zin = (j == 1) ? B.W0 : Z[chebz(j - 1)];
         const float* win = (j == 1) ? B.W0 : B.W1;
-        auto fn = k_cheb_step<false, MW>;
-        fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j,
-                                                         c->d_st, c->d_part);
-        CF_LAUNCH();
+        if (!spmv_default(c))
+        {
+            CF_TRY(launch_cheb_step_v(c, false, B, zin, win, B.W1, Z[chebz(j)], j));
+        }
+        else
+        {
+            auto fn = k_cheb_step<false, MW>;
+            fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)],
+                                                             j, c->d_st, c->d_part);
+            CF_LAUNCH();
+        }
         out = Z[chebz(j)];
     }
     k_scatter_f32<<<g, NT, 0, s>>>(n, c->d_perm, out, c->d_io32);
@@ -730,6 +767,8 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
         {
             case CF_KERNEL_CHEB_STEP:
             {
+                if (!spmv_default(c))
+                    return launch_cheb_step_v(c, false, B, B.Z0, B.W1, B.W1, B.Z1, 2);
                 auto fn = k_cheb_step<false, MW>;
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2,
                                                                  c->d_st, c->d_part);
@@ -737,6 +776,8 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             }
             case CF_KERNEL_SPMV32:
             {
+                if (!spmv_default(c))
+                    return launch_spmv32_v(c, B.diag, B.Z0, B.W0, B.Z1, c->d_scratch64);
                 auto fn = k_spmv32<MW>;
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B.diag, B.Z0, B.W0, B.Z1,
                                                                  c->d_scratch64,
@@ -745,6 +786,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             }
             case CF_KERNEL_PCG_P_SPMV:
             {
+                if (!spmv_default(c)) return launch_pcg_p_spmv_v(c, B, B.Z0);
                 auto fn = k_pcg_p_spmv<MW>;
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, c->d_st, c->d_part);
                 break;
