@@ -440,6 +440,109 @@ def run_multi_rhs(local, stream, steps=3):
             "converged": all(p.converged for p in res["m"])}
 
 
+def run_small_configs(local, stream, steps=20):
+    """The other single-GPU configurations, inputs resident:
+    C1 2-D Poisson 128^2 (Chebyshev order 4, deflate auto, maxRestarts 4,
+    tolerance 1e-6; launch/latency-bound: L2 holds the whole working set),
+    graph-driven and host-synchronised (one device->host read per
+    iteration, the reference's loop structure); C3 3-D upwind 96^3 with
+    cudaPBiCGStab to 1e-8.  Returns the summary and the solutions (for the
+    FP64 error check of the CPU leg)."""
+    import torch
+
+    from metal4foam_b200 import _lib, mesh
+    dev = torch.device("cuda", local)
+    out, sols = {}, {}
+    cases = [("C1", mesh.poisson2d(128, 128), _lib.CF_SOLVER_PCG,
+              dict(chebyshevOrder=4, deflate="auto", maxRestarts=4, tolerance=1e-6), steps),
+             ("C3", mesh.upwind3d((96, 96, 96), seed=2), _lib.CF_SOLVER_PBICGSTAB,
+              dict(tolerance=1e-8, maxIter=5000), 3)]
+    for name, s, solver, kw, k in cases:
+        ctx = _lib.Context(local)
+        ctx.set_stream(stream.cuda_stream)
+        a = s.addr
+        ctx.set_topology(a.n, a.nf, *a.arrays())
+        d_diag = torch.from_numpy(s.diag).to(dev)
+        d_up = torch.from_numpy(s.upper).to(dev)
+        d_lo = None if s.lower is None else torch.from_numpy(s.lower).to(dev)
+        d_b = torch.from_numpy(s.source).to(dev)
+        d_x = torch.zeros(s.n, dtype=torch.float64, device=dev)
+        res = {}
+
+        def solve(graph):
+            o = _lib.default_options(graph=graph, **kw)
+
+            def run():
+                d_x.zero_()
+                ctx.set_coeffs_device(d_diag, d_up, d_lo)
+                res["p"] = ctx.solve_device(solver, d_x, d_b, o)
+            return run
+
+        solve(1)()
+        ms = time_cuda(solve(1), k, stream) / k
+        p = res["p"]
+        sols[name] = (s, d_x.cpu().numpy())
+        ms_h = time_cuda(solve(0), max(1, k // 4), stream) / max(1, k // 4)
+        ctx.close()
+        out[name] = {"workload": f"{s.name} ({s.n} cells, {s.nf} faces)",
+                     "solver": "cudaPCG" if solver == _lib.CF_SOLVER_PCG else "cudaPBiCGStab",
+                     "options": kw, "ms_per_solve": round(ms, 4),
+                     "solves_per_s": round(1e3 / ms, 2),
+                     "host_sync_ms_per_solve": round(ms_h, 4),
+                     "iterations": p.nIterations, "restarts": p.nRestarts,
+                     "final_residual": p.finalResidual, "residual_l2": p.residualL2,
+                     "converged": bool(p.converged)}
+    return out, sols
+
+
+def run_autotune_table(ctx, n, nf):
+    """Every SpMV launch shape timed on the default workload's matrix
+    (cf_autotune; the bench keeps running the default shape)."""
+    best, table = ctx.autotune(reps=20, apply=False)
+    by = b_spmv(n, nf)
+    return {"best": best.as_dict(),
+            "shapes": [dict(cfg, ms_per_launch=round(ms, 5),
+                            gbs_algorithmic=round(by / (ms * 1e-3) / 1e9, 1))
+                       for cfg, ms in table]}
+
+
+def cpu_small_configs(sols, budget_s):
+    """CPU path and FP64-oracle error for C1 and C3: OpenFOAM-semantics
+    FP64 PCG (DIC, serial; diagonal, all threads) on C1 and PBiCGStab
+    (diagonal, all threads: a full solve) on C3, timed to the same
+    tolerance; the GPU solutions against an FP64 Krylov solve converged to
+    ||r||_2 <= 1e-12 ||b||_2."""
+    from oracle import oracle as O
+    nt = host_threads()
+    out = {}
+    if "C1" in sols:
+        s, x = sols["C1"]
+        t0 = time.perf_counter()
+        _, pd = O.foam_pcg(s, "DIC", tolerance=1e-6, maxIter=20000, nthreads=1)
+        t_dic = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        _, pg = O.foam_pcg(s, "diagonal", tolerance=1e-6, maxIter=20000, nthreads=nt)
+        t_diag = time.perf_counter() - t0
+        xr, _ = O.cg64(s, tol=1e-12, nthreads=nt)
+        out["C1"] = {"dic_serial": {"ms_per_solve": round(1e3 * t_dic, 3),
+                                    "iterations": pd.nIterations, "cores": 1},
+                     "diagonal": {"ms_per_solve": round(1e3 * t_diag, 3),
+                                  "iterations": pg.nIterations, "cores": nt},
+                     "gpu_error_vs_fp64": float(np.max(np.abs(x - xr)) / np.max(np.abs(xr)))}
+    if "C3" in sols:
+        s, x = sols["C3"]
+        t0 = time.perf_counter()
+        _, pb = O.foam_pbicgstab(s, tolerance=1e-8, maxIter=20000, nthreads=nt)
+        t_b = time.perf_counter() - t0
+        xr, _ = O.cg64(s, tol=1e-12, nthreads=nt)
+        out["C3"] = {"pbicgstab_diagonal": {"ms_per_solve": round(1e3 * t_b, 2),
+                                            "solves_per_s": round(1.0 / t_b, 4),
+                                            "iterations": pb.nIterations,
+                                            "final_residual": pb.finalResidual, "cores": nt},
+                     "gpu_error_vs_fp64": float(np.max(np.abs(x - xr)) / np.max(np.abs(xr)))}
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -574,12 +677,17 @@ def run_ours(args, ws, rank, local):
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
+        sols = {}
         if not args.no_extras:
             out["batched"] = batched
             out["adjoint"] = run_adjoint(local, stream)
             out["multi_rhs"] = run_multi_rhs(local, stream)
+            out["configs"], sols = run_small_configs(local, stream)
+            out["autotune"] = run_autotune_table(ctx, n, nf)
         if ws == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(sysm, args.cpu_budget)
+            if sols:
+                out["cpu_baseline"]["configs"] = cpu_small_configs(sols, args.cpu_budget)
     ctx.close()
     return out
 

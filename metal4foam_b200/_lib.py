@@ -219,6 +219,7 @@ class Context:
         check(L.cf_context_create(C.byref(h), int(device)))
         self.h = h
         self._keep = {}
+        self.reorder = reorder
         check(L.cf_context_set_reorder(self.h, REORDER[reorder]))
 
     def close(self):

@@ -14,6 +14,7 @@
 #include <fenv.h>
 #include <map>
 #include <memory>
+#include <set>
 #include <sstream>
 #include <string>
 
@@ -196,6 +197,24 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     opts.verbose = cudaDict_.getOrDefault<bool>("verbose", false);
     opts.graph = cudaDict_.getOrDefault<bool>("graph", true);
     opts.stagnationLimit = cudaDict_.getOrDefault<label>("stagnationLimit", 0);
+
+    // autotune yes: time the SpMV launch shapes once per context (the mesh
+    // of a context does not change during a run) and keep the fastest
+    if (cudaDict_.getOrDefault<bool>("autotune", false))
+    {
+        static std::set<const cf_context*> tuned;
+        if (tuned.insert(ctx).second)
+        {
+            cf_spmv_config best;
+            check(cf_autotune(ctx, 20, 1, &best, nullptr, 0, nullptr), "cf_autotune");
+            if (opts.verbose)
+            {
+                Info<< "    " << solverName << " SpMV shape: layout " << best.layout
+                    << " rowsPerWarp " << best.rowsPerWarp << " blockSize "
+                    << best.blockSize << " rhsTile " << best.rhsTile << nl;
+            }
+        }
+    }
 
     cf_performance perf;
     check

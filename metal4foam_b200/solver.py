@@ -139,10 +139,14 @@ def backend_cache_clear():
     for ctx in _BACKENDS.values():
         ctx.close()
     _BACKENDS.clear()
+    _TUNED.clear()
 
 
 _CONTROL_KEYS = ("maxRestarts", "iterationsPerSync", "deflate", "chebyshevOrder",
-                 "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit")
+                 "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit", "autotune")
+
+# backends whose SpMV launch shape has been chosen (autotune yes)
+_TUNED: Dict[tuple, dict] = {}
 
 
 class cudaFoamSolver:
@@ -152,8 +156,10 @@ class cudaFoamSolver:
     ``relTol``, ``maxIter``, ``minIter`` and the optional sub-dictionary
     ``cuda`` (``metal`` is accepted too, so existing dictionaries work)
     with ``maxRestarts``, ``iterationsPerSync``, ``deflate``,
-    ``chebyshevOrder``, ``chebyshevRatio``, ``profile``, ``verbose``
-    and ``graph``.
+    ``chebyshevOrder``, ``chebyshevRatio``, ``profile``, ``verbose``,
+    ``graph``, ``stagnationLimit`` and ``autotune`` (pick the SpMV launch
+    shape by timing, once per mesh and device, cached on disk; see
+    :mod:`metal4foam_b200.autotune`).
     """
 
     typeName = "cudaFoamSolver"
@@ -219,6 +225,17 @@ class cudaFoamSolver:
         bk.set_topology(a.size(), a.lowerAddr().shape[0], a.lowerAddr(), a.upperAddr(),
                         a.ownerStartAddr(), a.losortAddr(), a.losortStartAddr())
         tconv = bk.set_coeffs(m.diag(), m.upper(), m._lower)
+        if self.subDict_.get("autotune", False):
+            key = (self.fieldName_, id(a), self.device_)
+            if key not in _TUNED:
+                from types import SimpleNamespace
+
+                from . import autotune
+                shape = SimpleNamespace(n=a.size(), nf=a.lowerAddr().shape[0],
+                                        lowerAddr=a.lowerAddr(), upperAddr=a.upperAddr())
+                _TUNED[key] = autotune.tuned_config(bk, shape)
+                if self.subDict_.get("verbose", False):
+                    print(f"    {self.typeName}: SpMV launch shape {_TUNED[key]}")
         solver = _lib.CF_SOLVER_PBICGSTAB if self.useBiCGStab else _lib.CF_SOLVER_PCG
         p = bk.solve(solver, psi, src, self.options())
         return solverPerformance(

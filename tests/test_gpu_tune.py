@@ -167,3 +167,33 @@ def test_config_validation_and_topology_change(require_gpu):
     y0, _ = ctx.spmv32(x, None)
     assert np.array_equal(y, y0)
     ctx.close()
+
+
+def test_solver_autotune_key_uses_cache(require_gpu, tmp_path, monkeypatch):
+    """autotune yes in the cuda sub-dictionary: the first solve on a mesh
+    times the shapes and caches the winner; a fresh backend on the same
+    mesh applies the cached shape without timing."""
+    import json
+
+    from metal4foam_b200 import autotune
+    from metal4foam_b200.solver import backend_cache_clear, cudaPCG, lduMatrix
+    path = tmp_path / "tune.json"
+    monkeypatch.setenv("CUDAFOAM_TUNE_CACHE", str(path))
+    s = mesh.varcoeff3d((30, 28, 26), seed=32, permute=True)
+    m = lduMatrix(s.addr, s.diag, s.upper)
+    ctl = {"solver": "cudaPCG", "tolerance": 1e-7, "cuda": {"autotune": True}}
+    psi = np.zeros(s.n)
+    p = cudaPCG("p", m, ctl).solve(psi, s.source)
+    assert p.converged
+    stored = json.loads(path.read_text())
+    assert len(stored) == 1
+    entry = next(iter(stored.values()))
+    backend_cache_clear()
+    sol = cudaPCG("p", m, ctl)
+    psi2 = np.zeros(s.n)
+    p2 = sol.solve(psi2, s.source)
+    assert p2.converged
+    assert json.loads(path.read_text()) == stored
+    assert sol.backend().spmv_config().as_dict() == entry["config"]
+    assert autotune.mesh_key(sol.backend().description, s.addr) in stored
+    backend_cache_clear()
