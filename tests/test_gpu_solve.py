@@ -245,3 +245,25 @@ def test_edge_breakdown_reports_singular(require_gpu):
     assert perf.singular
     assert not perf.converged
     backend_cache_clear()
+
+
+def test_bicgstab_where_fp32_reductions_break_down(require_gpu, oracle):
+    """Upwind 64^3 to 1e-8: the reference's algorithm, whose dot products
+    are folded in FP32, loses rA0.rA to cancellation (it falls from ~1e5 to
+    rounding noise and then to exactly 0) and stops with a breakdown after
+    55 iterations; the same iteration with FP64-accumulated reductions
+    converges and states its FP64 residual."""
+    s = mesh.upwind3d((64, 64, 64), seed=2)
+    ref = oracle.metal_solve(s, bicgstab=True, tolerance=1e-8, maxIter=5000)
+    assert ref.singular and not ref.converged
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, s.lower)
+    x = np.zeros(s.n)
+    p = ctx.solve(_lib.CF_SOLVER_PBICGSTAB, x, s.source,
+                  _lib.default_options(tolerance=1e-8, maxIter=5000))
+    assert p.converged and not p.singular and p.finalResidual < 1e-8
+    r = s.source - mesh.amul_numpy(s, x)
+    assert np.sum(np.abs(r)) / p.normFactor == pytest.approx(p.finalResidual, rel=1e-9)
+    ctx.close()
