@@ -353,7 +353,7 @@ int cf_time_kernel(cf_context* ctx, int32_t which, int32_t reps,
  * order (the products of a row are added one by one in the reference's
  * entry order), so A x is bit-identical across shapes; dot products fold
  * their partial sums in a shape-dependent order.  The default is SELL32,
- * 32 rows per warp, 256 threads, rhsTile 4.  The batched kernels
+ * 32 rows per warp, 256 threads, rhsTile 4, indexBits 16.  The batched kernels
  * (cf_batch_*) and the multi-RHS kernels always use the default shape. */
 enum
 {
@@ -367,6 +367,10 @@ typedef struct cf_spmv_config
     int32_t rowsPerWarp;
     int32_t blockSize;
     int32_t rhsTile;
+    int32_t indexBits;      /* SELL32 column stream: 16 (row-relative offsets,
+                               used when every column of the reordered matrix
+                               lies within 32767 rows of its row; otherwise
+                               the 32-bit stream) or 32; ignored for LDU     */
 } cf_spmv_config;
 
 typedef struct cf_tune_entry

@@ -73,11 +73,12 @@ dbl = C.c_double
 # (name, restype, argtypes) of every exported function
 class SpmvConfig(C.Structure):
     _fields_ = [("layout", C.c_int32), ("rowsPerWarp", C.c_int32), ("blockSize", C.c_int32),
-                ("rhsTile", C.c_int32)]
+                ("rhsTile", C.c_int32), ("indexBits", C.c_int32)]
 
     def as_dict(self):
         return {"layout": LAYOUT_NAMES[self.layout], "rowsPerWarp": self.rowsPerWarp,
-                "blockSize": self.blockSize, "rhsTile": self.rhsTile}
+                "blockSize": self.blockSize, "rhsTile": self.rhsTile,
+                "indexBits": self.indexBits}
 
 
 class TuneEntry(C.Structure):
@@ -90,9 +91,9 @@ LAYOUTS = {"sell32": CF_LAYOUT_SELL32, "ldu": CF_LAYOUT_LDU}
 LAYOUT_NAMES = {v: k for k, v in LAYOUTS.items()}
 
 
-def spmv_config(layout="sell32", rowsPerWarp=32, blockSize=256, rhsTile=4):
+def spmv_config(layout="sell32", rowsPerWarp=32, blockSize=256, rhsTile=4, indexBits=16):
     return SpmvConfig(LAYOUTS[layout] if isinstance(layout, str) else int(layout),
-                      int(rowsPerWarp), int(blockSize), int(rhsTile))
+                      int(rowsPerWarp), int(blockSize), int(rhsTile), int(indexBits))
 
 
 SIGNATURES = [

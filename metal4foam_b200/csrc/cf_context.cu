@@ -95,6 +95,7 @@ void free_topology(cf_context* c)
     c->hasCoeffs = false;
     c->n = c->nf = 0;
     c->lastLow = c->lastUpp = nullptr;
+    c->d_col16 = nullptr;
 }
 
 // Validate the five lduAddressing arrays (the bounds check the reference
@@ -246,7 +247,9 @@ int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
 
     const int32_t nslices = (n + SLICE - 1) / SLICE;
     L.sliceOff.assign(nslices + 1, 0);
-    long long nnzp = 0;
+    std::vector<int32_t> sw(nslices, 0);
+    long long nnzSell = 0;
+    int32_t wmax = 0;
     for (int32_t s = 0; s < nslices; ++s)
     {
         int32_t w = 0;
@@ -257,6 +260,22 @@ int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
             const int32_t i = perm[r];
             w = std::max(w, (own[i + 1] - own[i]) + (losS[i + 1] - losS[i]));
         }
+        sw[s] = w;
+        nnzSell += (long long)w * SLICE;
+        wmax = std::max(wmax, w);
+    }
+    // one width for every slice when that pads at most 1/16 more entries:
+    // slice s then starts at 32 s W and the kernels need no sliceOff load
+    L.uniformW = 0;
+    if (wmax > 0 && (long long)nslices * SLICE * wmax <= nnzSell + nnzSell / 16)
+    {
+        L.uniformW = wmax;
+        for (int32_t s = 0; s < nslices; ++s) sw[s] = wmax;
+    }
+    long long nnzp = 0;
+    for (int32_t s = 0; s < nslices; ++s)
+    {
+        const int32_t w = sw[s];
         nnzp += (long long)w * SLICE;
         if (nnzp >= (1LL << 31) - 64)
             return fail(CF_ERR_TOO_LARGE, "matrix too large for 32-bit entry offsets");
@@ -320,6 +339,8 @@ DevSell sell_of(const cf_context* c)
     A.col = c->d_col;
     A.val = c->d_val32;
     A.val64 = c->d_val64;
+    A.col16 = c->cfgIndexBits == 16 ? c->d_col16 : nullptr;
+    A.ellW = c->ellW;
     return A;
 }
 
@@ -536,6 +557,7 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
     c->nslices = nslices;
     c->nnzp = nnzp;
     c->maxRowLen = maxw;
+    c->ellW = L.uniformW;
     c->perm = perm;
     c->identityPerm = !rcm;
     const size_t N = (size_t)n;
@@ -592,6 +614,37 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
                                 c->stream));
         CF_CUDA(cudaMemcpyAsync(c->d_upp, upp, sizeof(int32_t) * nf, cudaMemcpyHostToDevice,
                                 c->stream));
+    }
+    // compact column stream (row-relative 16-bit offsets) when every column
+    // lies within 32767 rows of its row (the host copy lives until the
+    // synchronisation below)
+    std::vector<short> col16((size_t)std::max(nnzp, 1LL), COL16_PAD);
+    {
+        bool fits = true;
+        for (int32_t sl = 0; sl < nslices && fits; ++sl)
+        {
+            const int32_t b0 = sliceOff[sl];
+            const int32_t w = (sliceOff[sl + 1] - b0) / SLICE;
+            for (int32_t k = 0; k < w && fits; ++k)
+                for (int32_t l = 0; l < SLICE; ++l)
+                {
+                    const int32_t e = b0 + SLICE * k + l;
+                    if (col[e] == -1) continue;
+                    const long long off = (long long)(col[e] & 0x7fffffff) - (long long)(sl * SLICE + l);
+                    if (off < -32767 || off > 32767)
+                    {
+                        fits = false;
+                        break;
+                    }
+                    col16[e] = (short)off;
+                }
+        }
+        if (fits)
+        {
+            CF_TRY(dalloc(c, &c->d_col16, col16.size()));
+            CF_CUDA(cudaMemcpyAsync(c->d_col16, col16.data(), sizeof(short) * col16.size(),
+                                    cudaMemcpyHostToDevice, c->stream));
+        }
     }
     CF_CUDA(cudaMemsetAsync(c->d_D, 0, sizeof(float) * 3 * N, c->stream));
     CF_CUDA(cudaStreamSynchronize(c->stream));

@@ -34,6 +34,7 @@ struct cf_context
     int reorderMode = 2;                   // CF_REORDER_AUTO
     int topoReorderMode = -1;
     int n = 0, nf = 0, nslices = 0, maxRowLen = 0;
+    int ellW = 0;                          // uniform slice width, 0 if the widths differ
     long long nnzp = 0;
     const int32_t* lastLow = nullptr;
     const int32_t* lastUpp = nullptr;
@@ -42,6 +43,7 @@ struct cf_context
     std::vector<void*> topoAllocs;
     int* d_sliceOff = nullptr;
     int* d_col = nullptr;
+    short* d_col16 = nullptr;              // row-relative columns, when they fit in 16 bits
     int* d_eface = nullptr;
     int* d_perm = nullptr;
     int* d_low = nullptr;
@@ -111,6 +113,7 @@ struct cf_context
     int cfgRowsPerWarp = 32;
     int cfgBlockSize = 256;
     int cfgRhsTile = 4;
+    int cfgIndexBits = 16;      // SELL-32 column stream: 16 (when built) or 32
     // the reference's addressing read directly (CF_LAYOUT_LDU), built on
     // first use; topology-lifetime allocations
     bool lduReady = false;
@@ -137,6 +140,7 @@ struct HostLayout
     int32_t nslices = 0;
     long long nnzp = 0;
     int32_t maxw = 0;
+    int32_t uniformW = 0;           // every slice this wide (0: widths differ)
 };
 
 int check_addressing(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,

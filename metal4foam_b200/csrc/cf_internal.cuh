@@ -36,6 +36,13 @@ constexpr int NPART = 4;           // reduction slots per kernel
 constexpr int STAG_LIMIT = 50;     // metalFoamBackend.C:606
 constexpr double VSMALL = 1.0e-300;
 
+// Column offsets of the compact index stream: entry e of row r holds
+// col - r in 16 bits (padding COL16_PAD).  Built when every column of the
+// reordered matrix lies within 32767 rows of its row (RCM keeps a 3-D mesh's
+// bandwidth near one plane of cells); it halves the index bytes of the FP32
+// SpMVs and names the same columns, so every sum is unchanged.
+constexpr short COL16_PAD = -32768;
+
 struct DevSell
 {
     int n;                          // rows
@@ -44,6 +51,9 @@ struct DevSell
     const int* col;                 // [nnz_padded]
     const float* val;               // [nnz_padded]
     const double* val64;            // [nnz_padded]
+    const short* col16 = nullptr;   // [nnz_padded] row-relative columns, or null
+    int ellW = 0;                   // > 0: every slice has this width and slice s
+                                    // starts at 32 s ellW (no sliceOff load)
 };
 
 // State of one inner solve (metalFoamBackend::Stats plus the device scalars

@@ -190,9 +190,48 @@ __device__ __forceinline__ float row_f32(const DevSell& A, int row, float acc,
                                          XF xf)
 {
     const int s = row >> 5;
-    const int b0 = __ldg(A.sliceOff + s);
-    const int w = (__ldg(A.sliceOff + s + 1) - b0) >> 5;
+    const int b0 = A.ellW ? s * SLICE * A.ellW : __ldg(A.sliceOff + s);
+    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + s + 1) - b0) >> 5;
     const int base = b0 + (row & 31);
+    if (A.col16)
+    {
+        // compact index stream: same columns, same order, half the bytes
+        if (w <= MAXW)
+        {
+            short o[MAXW];
+            float v[MAXW];
+#pragma unroll
+            for (int k = 0; k < MAXW; ++k)
+            {
+                if (k < w)
+                {
+                    o[k] = __ldcs(A.col16 + base + SLICE * k);
+                    v[k] = __ldcs(A.val + base + SLICE * k);
+                }
+                else
+                {
+                    o[k] = COL16_PAD;
+                    v[k] = 0.0f;
+                }
+            }
+            float x[MAXW];
+#pragma unroll
+            for (int k = 0; k < MAXW; ++k) x[k] = (o[k] != COL16_PAD) ? xf(row + o[k]) : 0.0f;
+#pragma unroll
+            for (int k = 0; k < MAXW; ++k)
+                if (o[k] != COL16_PAD) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
+        }
+        else
+        {
+            for (int k = 0; k < w; ++k)
+            {
+                const short o = __ldcs(A.col16 + base + SLICE * k);
+                if (o != COL16_PAD)
+                    acc = __fadd_rn(acc, __fmul_rn(__ldcs(A.val + base + SLICE * k), xf(row + o)));
+            }
+        }
+        return acc;
+    }
     if (w <= MAXW)
     {
         int c[MAXW];
@@ -239,8 +278,8 @@ __device__ __forceinline__ double row_f64(const DevSell& A, const double* vals,
                                           int row, double acc, XF xf)
 {
     const int s = row >> 5;
-    const int b0 = __ldg(A.sliceOff + s);
-    const int w = (__ldg(A.sliceOff + s + 1) - b0) >> 5;
+    const int b0 = A.ellW ? s * SLICE * A.ellW : __ldg(A.sliceOff + s);
+    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + s + 1) - b0) >> 5;
     const int base = b0 + (row & 31);
     if (w <= MAXW)
     {

@@ -539,6 +539,7 @@ int ensure_ldu(cf_context* c)
 
 bool valid_config(const cf_spmv_config& k)
 {
+    if (k.indexBits != 16 && k.indexBits != 32) return false;
     if (k.blockSize != 128 && k.blockSize != 256 && k.blockSize != 512) return false;
     if (k.rhsTile < 1 || k.rhsTile > 4) return false;
     if (k.layout == CF_LAYOUT_SELL32) return k.rowsPerWarp == 32;
@@ -595,17 +596,19 @@ cf_spmv_config config_of(const cf_context* c)
     k.rowsPerWarp = c->cfgRowsPerWarp;
     k.blockSize = c->cfgBlockSize;
     k.rhsTile = c->cfgRhsTile;
+    k.indexBits = c->cfgIndexBits;
     return k;
 }
 
 void apply_config(cf_context* c, const cf_spmv_config& k)
 {
     const bool shapeChanged = k.layout != c->cfgLayout || k.rowsPerWarp != c->cfgRowsPerWarp ||
-                              k.blockSize != c->cfgBlockSize;
+                              k.blockSize != c->cfgBlockSize || k.indexBits != c->cfgIndexBits;
     c->cfgLayout = k.layout;
     c->cfgRowsPerWarp = k.rowsPerWarp;
     c->cfgBlockSize = k.blockSize;
     c->cfgRhsTile = k.rhsTile;
+    c->cfgIndexBits = k.indexBits;
     if (shapeChanged)
     {
         // captured inner loops hold the previous shape's kernels
@@ -763,6 +766,7 @@ extern "C" int cf_spmv_config_default(cf_spmv_config* k)
     k->rowsPerWarp = 32;
     k->blockSize = NT;
     k->rhsTile = 4;
+    k->indexBits = 16;
     return CF_OK;
 }
 
@@ -780,7 +784,8 @@ extern "C" int cf_set_spmv_config(cf_context* c, const cf_spmv_config* k)
     if (!valid_config(*k))
         return fail(CF_ERR_UNSUPPORTED,
                     "SpMV configuration not offered (layout SELL32: rowsPerWarp 32; layout LDU: "
-                    "rowsPerWarp 32, 8, 4 or 1; blockSize 128, 256 or 512; rhsTile 1..4)");
+                    "rowsPerWarp 32, 8, 4 or 1; blockSize 128, 256 or 512; rhsTile 1..4; "
+                    "indexBits 16 or 32)");
     if (k->layout == CF_LAYOUT_LDU)
     {
         if (!c->hasTopo) return fail(CF_ERR_NO_TOPOLOGY, "cf_set_topology has not been called");
@@ -810,9 +815,15 @@ extern "C" int cf_autotune(cf_context* c, int32_t reps, int32_t apply, cf_spmv_c
     CF_TRY(launched(c));
 
     std::vector<cf_spmv_config> cand;
-    for (int bs : {128, 256, 512}) cand.push_back({CF_LAYOUT_SELL32, 32, bs, saved.rhsTile});
+    for (int bits : {16, 32})
+    {
+        if (bits == 16 && !c->d_col16) continue;   // offsets do not fit: no compact stream
+        for (int bs : {128, 256, 512})
+            cand.push_back({CF_LAYOUT_SELL32, 32, bs, saved.rhsTile, bits});
+    }
     for (int rpw : {32, 8, 4, 1})
-        for (int bs : {128, 256, 512}) cand.push_back({CF_LAYOUT_LDU, rpw, bs, saved.rhsTile});
+        for (int bs : {128, 256, 512})
+            cand.push_back({CF_LAYOUT_LDU, rpw, bs, saved.rhsTile, 32});
     int nt = 0;
     double bestMs = 1e300;
     cf_spmv_config win = saved;

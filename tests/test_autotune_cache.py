@@ -45,7 +45,8 @@ def test_tune_once_then_cached(tmp_path, monkeypatch):
     ctx = FakeContext()
     cfg = autotune.tuned_config(ctx, addr)
     assert ctx.tuned == 1 and ctx.applied == []
-    assert cfg == {"layout": "ldu", "rowsPerWarp": 8, "blockSize": 128, "rhsTile": 3}
+    assert cfg == {"layout": "ldu", "rowsPerWarp": 8, "blockSize": 128, "rhsTile": 3,
+                   "indexBits": 16}
     stored = json.loads(path.read_text())
     (key, entry), = stored.items()
     assert key == autotune.mesh_key(ctx.description, addr)

@@ -10,8 +10,8 @@ from metal4foam_b200 import _lib, mesh
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = ([("sell32", 32, bs) for bs in (128, 256, 512)] +
-          [("ldu", rpw, bs) for rpw in (32, 8, 4, 1) for bs in (128, 256, 512)])
+SHAPES = ([("sell32", 32, bs, bits) for bits in (16, 32) for bs in (128, 256, 512)] +
+          [("ldu", rpw, bs, 32) for rpw in (32, 8, 4, 1) for bs in (128, 256, 512)])
 
 
 def make_ctx(s, reorder="auto"):
@@ -37,10 +37,10 @@ def test_spmv_bitwise_across_shapes(require_gpu, oracle, kind):
     y0, d0 = ctx.spmv32(x, w)
     yr, _ = oracle.Ldu32View(s).spmv(x, w)
     assert np.array_equal(y0, yr)           # the reference kernel's arithmetic
-    for layout, rpw, bs in SHAPES:
-        ctx.set_spmv_config(layout=layout, rowsPerWarp=rpw, blockSize=bs)
+    for layout, rpw, bs, bits in SHAPES:
+        ctx.set_spmv_config(layout=layout, rowsPerWarp=rpw, blockSize=bs, indexBits=bits)
         y, d = ctx.spmv32(x, w)
-        assert np.array_equal(y, y0), (layout, rpw, bs)
+        assert np.array_equal(y, y0), (layout, rpw, bs, bits)
         assert d == pytest.approx(d0, rel=1e-12, abs=1e-12)
     ctx.close()
 
@@ -50,9 +50,9 @@ def test_cheb_apply_bitwise_across_shapes(require_gpu):
     ctx = make_ctx(s)
     r = np.random.default_rng(4).standard_normal(s.n).astype(np.float32)
     z0 = ctx.cheb_apply(r, 6, 2.0)
-    for layout, rpw, bs in SHAPES:
-        ctx.set_spmv_config(layout=layout, rowsPerWarp=rpw, blockSize=bs)
-        assert np.array_equal(ctx.cheb_apply(r, 6, 2.0), z0), (layout, rpw, bs)
+    for layout, rpw, bs, bits in SHAPES:
+        ctx.set_spmv_config(layout=layout, rowsPerWarp=rpw, blockSize=bs, indexBits=bits)
+        assert np.array_equal(ctx.cheb_apply(r, 6, 2.0), z0), (layout, rpw, bs, bits)
     ctx.close()
 
 
@@ -122,7 +122,7 @@ def test_autotune_picks_a_timed_shape(require_gpu):
     assert all(ms > 0 for _, ms in table)
     fastest = min(table, key=lambda t: t[1])[0]
     b = best.as_dict()
-    keys = ("layout", "rowsPerWarp", "blockSize")
+    keys = ("layout", "rowsPerWarp", "blockSize", "indexBits")
     assert {k: b[k] for k in keys} == {k: fastest[k] for k in keys}
     assert 1 <= b["rhsTile"] <= 4
     assert ctx.spmv_config().as_dict() == b
@@ -197,3 +197,38 @@ def test_solver_autotune_key_uses_cache(require_gpu, tmp_path, monkeypatch):
     assert sol.backend().spmv_config().as_dict() == entry["config"]
     assert autotune.mesh_key(sol.backend().description, s.addr) in stored
     backend_cache_clear()
+
+
+def test_compact_columns_fall_back_when_offsets_do_not_fit(require_gpu, oracle):
+    """A randomly numbered mesh below the RCM threshold keeps columns far
+    from their rows: no 16-bit stream is built, indexBits 16 runs the 32-bit
+    stream and the autotuner offers only 32-bit SELL shapes."""
+    s = mesh.varcoeff3d((40, 40, 40), seed=33, permute=True)      # 64,000 cells
+    ctx = make_ctx(s)
+    x = np.random.default_rng(8).standard_normal(s.n).astype(np.float32)
+    y16, _ = ctx.spmv32(x, None)
+    ctx.set_spmv_config(indexBits=32)
+    y32, _ = ctx.spmv32(x, None)
+    yr, _ = oracle.Ldu32View(s).spmv(x)
+    assert np.array_equal(y16, yr) and np.array_equal(y32, yr)
+    _, table = ctx.autotune(reps=3, apply=False)
+    assert all(t["indexBits"] == 32 for t, _ in table)
+    assert len(table) == len(SHAPES) - 3
+    ctx.close()
+
+
+def test_pcg_solve_bitwise_with_either_column_stream(require_gpu):
+    """The default shape with 16- or 32-bit columns is the same computation."""
+    s = mesh.varcoeff3d((26, 25, 24), seed=34, permute=True)
+    ctx = _lib.Context(0, "rcm")
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, None)
+    out = []
+    for bits in (16, 32):
+        ctx.set_spmv_config(indexBits=bits)
+        x = np.zeros(s.n)
+        p = ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, _lib.default_options(tolerance=1e-8))
+        out.append((x, p.nIterations, p.finalResidual))
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1:] == out[1][1:]
+    ctx.close()
