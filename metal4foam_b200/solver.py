@@ -251,6 +251,43 @@ class cudaFoamSolver:
     def solve(self, psi, source, cmpt: int = 0) -> solverPerformance:
         return self.solveImpl(psi, source, cmpt)
 
+    def solveSegregated(self, psi: np.ndarray, source: np.ndarray):
+        """All components of a vector equation on this matrix at once
+        (fvMatrix<vector>::solveSegregated calls the scalar solver per
+        component; here every SpMV serves all components): psi and source
+        are C-contiguous float64 (nComponents, nCells), psi updated in place.
+        Returns one solverPerformance per component, each equal to what
+        solve() returns for that component alone.  cudaPBiCGStab only."""
+        if not self.useBiCGStab:
+            raise FatalError(f"{self.typeName}: segregated multi-component solves are "
+                             "cudaPBiCGStab (momentum)")
+        if any(i is not None for i in self.interfaces_):
+            raise FatalError(f"{self.typeName} does not support coupled boundaries "
+                             "(processor/cyclic/AMI); run serially on a mesh without coupled "
+                             "patches.")
+        if (not isinstance(psi, np.ndarray) or psi.dtype != np.float64 or psi.ndim != 2
+                or not psi.flags["C_CONTIGUOUS"]):
+            raise TypeError("psi must be a C-contiguous float64 (nComponents, nCells) array")
+        src = np.ascontiguousarray(source, np.float64)
+        if src.shape != psi.shape:
+            raise ValueError("psi and source shapes differ")
+        m = self.matrix_
+        a = m.lduAddr()
+        bk = self.backend()
+        bk.set_topology(a.size(), a.lowerAddr().shape[0], a.lowerAddr(), a.upperAddr(),
+                        a.ownerStartAddr(), a.losortAddr(), a.losortStartAddr())
+        bk.set_coeffs(m.diag(), m.upper(), m._lower)
+        out = []
+        for k, p in enumerate(bk.solve_multi(_lib.CF_SOLVER_PBICGSTAB, psi, src, self.options())):
+            out.append(solverPerformance(
+                solverName=self.typeName, fieldName=f"{self.fieldName_}.component({k})",
+                initialResidual=p.initialResidual, finalResidual=p.finalResidual,
+                nIterations=p.nIterations, converged=bool(p.converged),
+                singular=bool(p.singular), nRestarts=p.nRestarts, stagnated=bool(p.stagnated),
+                normFactor=p.normFactor, residualL2=p.residualL2,
+                timings=dict(tSolve=p.tSolve)))
+        return out
+
     def scalarSolve(self, psi, source, cmpt: int = 0) -> solverPerformance:
         return self.solveImpl(psi, source, cmpt)
 

@@ -193,3 +193,26 @@ def test_momentum_64cube_three_components(require_gpu):
         r = rhs[k] - mesh.amul_numpy(s, psi[k])
         assert np.sum(np.abs(r)) / perfs[k].normFactor < 1.01e-6
     ctx.close()
+
+
+def test_solver_surface_segregated(require_gpu):
+    """cudaPBiCGStab.solveSegregated: every component equals solve() on it."""
+    from metal4foam_b200.solver import (FatalError, backend_cache_clear, cudaPBiCGStab,
+                                        cudaPCG, lduMatrix)
+    s = mesh.upwind3d((18, 16, 14), seed=40)
+    m = lduMatrix(s.addr, s.diag, s.upper, s.lower)
+    ctl = {"solver": "cudaPBiCGStab", "tolerance": 1e-8}
+    b = rhs_set(s, 3, 41)
+    psi = np.zeros((3, s.n))
+    perfs = cudaPBiCGStab("U", m, ctl).solveSegregated(psi, b)
+    for k in range(3):
+        x = np.zeros(s.n)
+        p1 = cudaPBiCGStab("U", m, ctl).solve(x, b[k])
+        assert np.array_equal(psi[k], x)
+        assert perfs[k].nIterations == p1.nIterations and perfs[k].converged
+        assert perfs[k].fieldName == f"U.component({k})"
+    with pytest.raises(FatalError):
+        sym = mesh.varcoeff3d((6, 5, 4), seed=1)
+        cudaPCG("p", lduMatrix(sym.addr, sym.diag, sym.upper), {"solver": "cudaPCG"}) \
+            .solveSegregated(np.zeros((2, sym.n)), np.zeros((2, sym.n)))
+    backend_cache_clear()

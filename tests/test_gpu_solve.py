@@ -267,3 +267,36 @@ def test_bicgstab_where_fp32_reductions_break_down(require_gpu, oracle):
     r = s.source - mesh.amul_numpy(s, x)
     assert np.sum(np.abs(r)) / p.normFactor == pytest.approx(p.finalResidual, rel=1e-9)
     ctx.close()
+
+
+def _edge_system(n, low, upp, diag, upper, src):
+    a = mesh.ldu_addressing(n, np.array(low, np.int32), np.array(upp, np.int32))
+    return mesh.LduSystem("edge", a, np.asarray(diag, float), np.asarray(upper, float), None,
+                          np.asarray(src, float), np.zeros(n))
+
+
+@pytest.mark.parametrize("case", ["one_cell", "disconnected", "diagonal_only"])
+@pytest.mark.parametrize("solver", [_lib.CF_SOLVER_PCG, _lib.CF_SOLVER_PBICGSTAB])
+def test_edge_degenerate_meshes(require_gpu, oracle, case, solver):
+    """A single cell (no faces), cells without neighbours next to a coupled
+    chain, and a diagonal-only matrix: same iterations, flags and result as
+    the reference algorithm."""
+    if case == "one_cell":
+        s = _edge_system(1, [], [], [2.0], [], [4.0])
+    elif case == "disconnected":
+        s = _edge_system(5, [0, 1], [1, 2], [2.0, 3.0, 2.0, 5.0, 1.0], [-1.0, -1.0],
+                         [1.0, 2.0, 3.0, 4.0, 5.0])
+    else:
+        s = _edge_system(1000, [], [], np.linspace(1, 3, 1000), [], np.sin(np.arange(1000.0)))
+    ref = oracle.metal_solve(s, bicgstab=solver == _lib.CF_SOLVER_PBICGSTAB)
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, None)
+    x = np.zeros(s.n)
+    p = ctx.solve(solver, x, s.source, _lib.default_options())
+    assert p.converged == ref.converged and p.deflated == ref.deflated
+    assert p.nIterations == ref.nIterations and p.nRestarts == ref.nRestarts
+    xd = np.linalg.solve(mesh.to_csr(s).toarray(), s.source)
+    assert np.max(np.abs(x - xd)) <= 2 * max(np.max(np.abs(ref.psi - xd)), 1e-7) * np.max(np.abs(xd))
+    ctx.close()
