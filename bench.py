@@ -200,16 +200,35 @@ def cpu_path_sample(sysm, precond, nthreads, budget_s):
     return (time.perf_counter() - t0) / p.nIterations, p.nIterations
 
 
-def cpu_baseline(sysm, budget_s):
+def fp64_error(sysm, psi, sec_per_iter, budget_s):
+    """Error of the GPU solution against OpenFOAM-semantics FP64 PCG
+    (diagonal preconditioner, all host threads) converged to normalised
+    residual 1e-12, when about 3500 iterations fit in budget_s; else None."""
+    if psi is None or sec_per_iter * 3500 > budget_s:
+        return None
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    xr, p = O.foam_pcg(sysm, "diagonal", tolerance=1e-12, maxIter=8000,
+                       nthreads=host_threads())
+    return {"rel_max_error": float(np.max(np.abs(psi - xr)) / np.max(np.abs(xr))),
+            "reference": "FP64 PCG (diagonal), normalised residual "
+                         f"{p.finalResidual:.2e} after {p.nIterations} iterations",
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
+def cpu_baseline(sysm, budget_s, psi=None, error_budget_s=90.0):
     """Diagonal PCG on all host threads (the faster CPU configuration here)
     is the reported value; serial PCG+DIC (OpenFOAM's default, the
-    reference's own comparison) is reported beside it."""
+    reference's own comparison) is reported beside it, and the error of
+    the GPU solution psi against an FP64 solve to 1e-12."""
     nt = host_threads()
     sec_diag, it_diag = cpu_path_sample(sysm, "diagonal", nt, budget_s)
     sec_dic, it_dic = cpu_path_sample(sysm, "DIC", 1, min(budget_s, 8.0))
     v_diag = 1.0 / (sec_diag * CPU_ITERS["diagonal"])
     v_dic = 1.0 / (sec_dic * CPU_ITERS["DIC"])
+    err = fp64_error(sysm, psi, sec_diag, error_budget_s)
     return {
+        "gpu_error_vs_fp64": err,
         "value": round(v_diag, 6), "unit": "solves/s", "cores": nt, "kind": "port",
         "sample": (f"OpenFOAM-semantics FP64 PCG, diagonal preconditioner, {nt} OpenMP threads "
                    f"(oracle/foam_cpu.c) on the full 128^3 system: {it_diag} iterations timed "
@@ -592,6 +611,7 @@ def run_ours(args, ws, rank, local):
     launches = ctx.kernel_launches() - launches0
     ms_max = max_over_ranks(ms, ws)
     ok = all(p.converged and p.finalResidual < 1e-6 for p in perfs)
+    psi_out = d_psi.cpu().numpy()
     iters = [p.nIterations for p in perfs]
     last = perfs[-1]
 
@@ -685,7 +705,8 @@ def run_ours(args, ws, rank, local):
             out["configs"], sols = run_small_configs(local, stream)
             out["autotune"] = run_autotune_table(ctx, n, nf)
         if ws == 1 and not args.no_cpu:
-            out["cpu_baseline"] = cpu_baseline(sysm, args.cpu_budget)
+            out["cpu_baseline"] = cpu_baseline(sysm, args.cpu_budget, psi_out,
+                                               args.error_budget)
             if sols:
                 out["cpu_baseline"]["configs"] = cpu_small_configs(sols, args.cpu_budget)
     ctx.close()
@@ -736,6 +757,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-budget", type=float, default=12.0,
                     help="seconds of CPU work for the CPU-baseline sample")
+    ap.add_argument("--error-budget", type=float, default=90.0,
+                    help="largest estimated CPU time for the FP64 reference solve of the "
+                         "error check (skipped when longer)")
     ap.add_argument("--ref-step-seconds", type=float, default=5.0,
                     help="CPU seconds per step of --impl reference")
     ap.add_argument("--no-cpu", action="store_true")
