@@ -97,6 +97,12 @@ typedef struct
     int32_t stagnationLimit;   /* inner iterations without a new minimum of
                                   sum|r| before the inner solve stops; 0
                                   (default) = 50, metalFoamBackend.C:606   */
+    int32_t persistentMaxCells;/* with graph = 1: meshes up to this many
+                                  cells run each inner solve as ONE
+                                  cooperative kernel (grid barriers between
+                                  the phases of an iteration, bit-identical
+                                  results); 0 (default) = 262144, < 0 =
+                                  never                                    */
 } cf_options;
 
 /* solverPerformance plus the reference's profile/verbose figures

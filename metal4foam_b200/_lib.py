@@ -46,6 +46,7 @@ class Options(C.Structure):
         ("deflate", C.c_int32), ("chebyshevOrder", C.c_int32), ("chebyshevRatio", C.c_double),
         ("profile", C.c_int32), ("verbose", C.c_int32), ("graph", C.c_int32),
         ("stagnationLimit", C.c_int32),
+        ("persistentMaxCells", C.c_int32),
     ]
 
 

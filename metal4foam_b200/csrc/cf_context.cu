@@ -431,6 +431,7 @@ extern "C" int cf_context_create(cf_context** out, int32_t device)
     c->numSMs = prop.multiProcessorCount;
     c->maxBlocksPerSM = std::max(1, prop.maxThreadsPerMultiProcessor / NT);
     c->maxCtasPerSM = std::max(c->maxBlocksPerSM, prop.maxBlocksPerMultiProcessor);
+    c->coopLaunch = prop.cooperativeLaunch != 0;
     c->l2Bytes = prop.l2CacheSize;
     cudaError_t e = cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking);
     if (e != cudaSuccess)
@@ -447,6 +448,7 @@ extern "C" int cf_context_create(cf_context** out, int32_t device)
         cudaMalloc((void**)&c->d_drv, sizeof(DriverState)) != cudaSuccess ||
         cudaMalloc((void**)&c->d_chebC, sizeof(float) * 2 * CF_MAX_CHEB) != cudaSuccess ||
         cudaMalloc((void**)&c->d_scratch64, sizeof(double) * 4) != cudaSuccess ||
+        cudaMalloc((void**)&c->d_bar, sizeof(unsigned int) * 4) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_st, sizeof(InnerState)) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_drv, sizeof(DriverState)) != cudaSuccess)
     {
@@ -481,6 +483,7 @@ extern "C" int cf_context_destroy(cf_context* c)
     if (c->d_drv) cudaFree(c->d_drv);
     if (c->d_chebC) cudaFree(c->d_chebC);
     if (c->d_scratch64) cudaFree(c->d_scratch64);
+    if (c->d_bar) cudaFree(c->d_bar);
     if (c->h_st) cudaFreeHost(c->h_st);
     if (c->h_drv) cudaFreeHost(c->h_drv);
     if (c->ev0) cudaEventDestroy(c->ev0);

@@ -109,6 +109,8 @@ struct cf_context
     // SpMV launch shape of the FP32 Krylov kernels (cf_tune.cu): layout
     // (CF_LAYOUT_*), rows per warp, block size, multi-RHS tile
     int maxCtasPerSM = 32;
+    bool coopLaunch = false;               // device supports cooperative launches
+    unsigned int* d_bar = nullptr;         // grid barrier of persistent inner solves: count, generation, error
     int cfgLayout = 0;
     int cfgRowsPerWarp = 32;
     int cfgBlockSize = 256;
@@ -174,5 +176,12 @@ int launch_bicg_b_v(cf_context* c, const BicgBufs& B);
 int launch_bicg_d_v(cf_context* c, const BicgBufs& B);
 int launch_spmv32_v(cf_context* c, const float* diag, const float* x, const float* w, float* y,
                     double* out);
+
+// Inner solve as one cooperative kernel (cf_persist.cu) when the mesh has
+// at most maxCells cells (0: 262144, < 0: never) and the launch fits;
+// *ran tells whether it was launched.  persistent_status reads the grid
+// barrier's error word after the stream has completed.
+int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran);
+int persistent_status(cf_context* c);
 
 }  // namespace cf

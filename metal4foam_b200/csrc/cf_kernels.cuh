@@ -781,7 +781,10 @@ static __global__ void __launch_bounds__(NT) k_pcg_p_spmv(DevSell A, PcgBufs B, 
 // End-of-iteration bookkeeping of metalFoamBackend::pcg (.C:676-715) on the
 // device: breakdown, minimum-residual iterate, convergence, stagnation, at
 // every batch boundary of iterationsPerSync.
-__device__ __forceinline__ void inner_sync_point(InnerState* st, bool checkWApA)
+// (S = InnerState, or volatile InnerState inside a persistent kernel, whose
+// state must not be served from a stale L1 line)
+template <class S>
+__device__ __forceinline__ void inner_sync_point(S* st, bool checkWApA)
 {
     const int it = st->it;
     const bool sync = (it - st->lastSync >= st->ips) || (it >= st->maxIter);

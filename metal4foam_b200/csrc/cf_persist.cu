@@ -1,0 +1,451 @@
+// cf_persist.cu -- the inner PCG / BiCGStab loop of a small mesh as ONE
+// cooperative kernel.
+//
+// For meshes whose rows fit one per thread in a co-resident grid, the
+// phases of an iteration (Chebyshev steps, p-update SpMV, update; or the
+// five BiCGStab phases) run inside one launch separated by grid barriers,
+// and the launch loops until the device-side stopping tests end the inner
+// solve -- no kernel launch and no graph node per phase.  Each phase is the
+// arithmetic of the corresponding kernel of cf_kernels.cuh on the same
+// grid (one row per thread, ceil(n / 256) blocks), and the reductions are
+// the same last-block folds, so a persistent inner solve returns exactly
+// what the graph-driven one returns.
+//
+// Inside one launch, L1 is not coherent across SMs: every load of data that
+// another block writes during the launch (vectors, partials, solver state)
+// bypasses L1 (ld.global.cg, volatile state); data constant during the
+// launch (matrix, diagonals, Chebyshev constants) keeps the read-only path.
+//
+// Grid barrier: generation counter in global memory; the last block to
+// arrive resets the count and bumps the generation.  Every wait is bounded
+// (kBarrierSpins polls with a short sleep); a block that gives up sets the
+// error word and leaves, the others leave at their next barrier, and the
+// host reports CF_ERR_DEVICE_TIMEOUT.  The launch is cooperative, so all
+// blocks are co-resident and the bound is never reached in normal runs.
+#include "cudafoam.h"
+#include "cf_host.hpp"
+
+#include <algorithm>
+#include <string>
+
+using namespace cf;
+
+namespace {
+
+constexpr unsigned long long kBarrierSpins = 1ull << 24;
+constexpr int MW = MAXW_UNROLL;
+
+struct Bar
+{
+    unsigned int* count;
+    unsigned int* gen;
+    int* err;
+};
+
+__device__ __forceinline__ bool grid_barrier(const Bar& b)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned int* vgen = b.gen;
+        const unsigned int g = *vgen;
+        __threadfence();
+        if (atomicAdd(b.count, 1u) == gridDim.x - 1)
+        {
+            *b.count = 0u;
+            __threadfence();
+            atomicAdd(b.gen, 1u);
+        }
+        else
+        {
+            unsigned long long spins = 0;
+            while (*vgen == g)
+            {
+                if (++spins > kBarrierSpins)
+                {
+                    atomicExch(b.err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int*)b.err == 0;
+}
+
+__device__ __forceinline__ float ld(const float* p) { return __ldcg(p); }
+
+// ---------------------------------------------------------------- PCG
+
+template <bool LAST>
+__device__ __forceinline__ void p_cheb_step(const DevSell& A, const PcgBufs& B, const float* zin,
+                                            const float* win, float* wout, float* zout, int j,
+                                            volatile InnerState* st, unsigned int* ticket,
+                                            double* part)
+{
+    const float c2 = __ldg(B.chebC + 2 * j - 1);
+    const float c3 = __ldg(B.chebC + 2 * j);
+    double acc[1] = {0.0};
+    CF_ROWS(row, A.n)
+    {
+        const float zr = ld(zin + row);
+        const float v = row_f32<MW>(A, row, __fmul_rn(__ldg(B.diag + row), zr),
+                                    [&](int c) { return ld(zin + c); });
+        const float r = ld(B.rA + row);
+        const float wn = __fadd_rn(__fmul_rn(c2, ld(win + row)),
+                                   __fmul_rn(__fmul_rn(c3, __ldg(B.rD + row)), __fsub_rn(r, v)));
+        const float zn = __fadd_rn(zr, wn);
+        wout[row] = wn;
+        zout[row] = zn;
+        if (LAST) acc[0] += (double)zn * (double)r;
+    }
+    if (LAST)
+    {
+        if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0)
+        {
+            st->wArAold = st->wArA;
+            st->wArA = acc[0];
+            st->beta = (st->it == 0) ? 0.0 : st->wArA / st->wArAold;
+        }
+    }
+}
+
+__device__ __forceinline__ void p_pcg_p_spmv(const DevSell& A, const PcgBufs& B, const float* wA,
+                                             volatile InnerState* st, unsigned int* ticket,
+                                             double* part)
+{
+    const int n = A.n;
+    const int par = st->it & 1;
+    const float* Pold = B.P + (size_t)(par ^ 1) * n;
+    float* Pn = B.P + (size_t)par * n;
+    const float beta = (float)st->beta;
+    auto pf = [&](int c) { return __fadd_rn(ld(wA + c), __fmul_rn(beta, ld(Pold + c))); };
+    double acc[1] = {0.0};
+    CF_ROWS(row, n)
+    {
+        const float pr = pf(row);
+        const float y = row_f32<MW>(A, row, __fmul_rn(__ldg(B.diag + row), pr), pf);
+        Pn[row] = pr;
+        B.Q[row] = y;
+        acc[0] += (double)pr * (double)y;
+    }
+    if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0)
+    {
+        st->wApA = acc[0];
+        st->alpha = st->wArA / st->wApA;
+    }
+}
+
+template <bool CHEB>
+__device__ __forceinline__ void p_pcg_update(const PcgBufs& B, volatile InnerState* st,
+                                             unsigned int* ticket, double* part)
+{
+    const int n = B.n;
+    const int par = st->it & 1;
+    const float* P = B.P + (size_t)par * n;
+    const float* D = B.D + (size_t)st->cur * n;
+    float* Dn = B.D + (size_t)st->nxt * n;
+    const float alpha = (float)st->alpha;
+    const float c1 = CHEB ? __ldg(B.chebC) : 0.0f;
+    double acc[2] = {0.0, 0.0};
+    CF_ROWS(row, n)
+    {
+        Dn[row] = __fadd_rn(ld(D + row), __fmul_rn(alpha, ld(P + row)));
+        const float rn = __fsub_rn(ld(B.rA + row), __fmul_rn(alpha, ld(B.Q + row)));
+        B.rA[row] = rn;
+        acc[0] += (double)fabsf(rn);
+        if (CHEB)
+        {
+            B.W0[row] = __fmul_rn(__fmul_rn(c1, __ldg(B.rD + row)), rn);
+        }
+        else
+        {
+            const float wa = __fmul_rn(rn, __ldg(B.rD + row));
+            B.W0[row] = wa;
+            acc[1] += (double)wa * (double)rn;
+        }
+    }
+    if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
+    {
+        st->res = acc[0];
+        if (!CHEB)
+        {
+            st->wArAold = st->wArA;
+            st->wArA = acc[1];
+            st->beta = st->wArA / st->wArAold;
+        }
+        st->cur = st->nxt;
+        st->it = st->it + 1;
+        inner_sync_point(st, true);
+    }
+}
+
+// launch_pcg_body's phases, repeated until the inner solve is done
+template <bool CHEB>
+__global__ void __launch_bounds__(NT) kp_pcg(DevSell A, PcgBufs B, int order, InnerState* stp,
+                                             double* part, Bar bar)
+{
+    volatile InnerState* st = stp;
+    unsigned int* ticket = &stp->ticket;
+    float* Z[2] = {B.Z0, B.Z1};
+    while (!st->done)
+    {
+        if (CHEB)
+        {
+            for (int j = 1; j < order; ++j)
+            {
+                const float* zin = (j == 1) ? B.W0 : Z[(j - 1) & 1];
+                const float* win = (j == 1) ? B.W0 : B.W1;
+                if (j == order - 1)
+                    p_cheb_step<true>(A, B, zin, win, B.W1, Z[j & 1], j, st, ticket, part);
+                else
+                    p_cheb_step<false>(A, B, zin, win, B.W1, Z[j & 1], j, st, ticket, part);
+                if (!grid_barrier(bar)) return;
+            }
+        }
+        p_pcg_p_spmv(A, B, CHEB ? Z[(order - 1) & 1] : B.W0, st, ticket, part);
+        if (!grid_barrier(bar)) return;
+        p_pcg_update<CHEB>(B, st, ticket, part);
+        if (!grid_barrier(bar)) return;
+    }
+}
+
+// ---------------------------------------------------------------- BiCGStab
+
+__device__ __forceinline__ void p_bicg_a(const BicgBufs& B, volatile InnerState* st)
+{
+    const float beta = (float)st->beta;
+    const float omega = (float)st->omega;
+    CF_ROWS(row, B.n)
+    {
+        const float p = __fadd_rn(ld(B.rA + row),
+                                  __fmul_rn(beta, __fsub_rn(ld(B.P + row), __fmul_rn(omega, ld(B.AyA + row)))));
+        B.P[row] = p;
+        B.yA[row] = __fmul_rn(__ldg(B.rD + row), p);
+    }
+}
+
+__device__ __forceinline__ void p_bicg_b(const DevSell& A, const BicgBufs& B,
+                                         volatile InnerState* st, unsigned int* ticket,
+                                         double* part)
+{
+    const float* yA = B.yA;
+    double acc[1] = {0.0};
+    CF_ROWS(row, A.n)
+    {
+        const float y = row_f32<MW>(A, row, __fmul_rn(__ldg(B.diag + row), ld(yA + row)),
+                                    [&](int c) { return ld(yA + c); });
+        B.AyA[row] = y;
+        acc[0] += (double)ld(B.rA0 + row) * (double)y;
+    }
+    if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0)
+    {
+        st->rA0AyA = acc[0];
+        st->alpha = st->rA0rA / st->rA0AyA;
+    }
+}
+
+__device__ __forceinline__ void p_bicg_c(const BicgBufs& B, volatile InnerState* st,
+                                         unsigned int* ticket, double* part)
+{
+    const float alpha = (float)st->alpha;
+    double acc[1] = {0.0};
+    CF_ROWS(row, B.n)
+    {
+        const float sv = __fsub_rn(ld(B.rA + row), __fmul_rn(alpha, ld(B.AyA + row)));
+        B.sA[row] = sv;
+        B.zA[row] = __fmul_rn(__ldg(B.rD + row), sv);
+        acc[0] += (double)fabsf(sv);
+    }
+    if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0)
+    {
+        st->resS = acc[0];
+        if (!isfinite(st->rA0rA) || !isfinite(st->alpha) || !isfinite(st->resS))
+        {
+            st->singular = 1;
+            st->done = 1;
+        }
+        else if (st->resS <= st->target)
+        {
+            st->early = 1;
+            st->done = 1;
+        }
+    }
+}
+
+__device__ __forceinline__ void p_bicg_d(const DevSell& A, const BicgBufs& B,
+                                         volatile InnerState* st, unsigned int* ticket,
+                                         double* part)
+{
+    const int n = A.n;
+    double acc[2] = {0.0, 0.0};
+    if (st->early)
+    {
+        if (st->converged) return;
+        const float alpha = (float)st->alpha;
+        const float* D = B.D + (size_t)st->cur * n;
+        float* Dn = B.D + (size_t)st->nxt * n;
+        CF_ROWS(row, n) Dn[row] = __fadd_rn(ld(D + row), __fmul_rn(alpha, ld(B.yA + row)));
+        if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
+        {
+            st->cur = st->nxt;
+            st->it = st->it + 1;
+            st->finalResSum = st->resS;
+            st->converged = 1;
+        }
+        return;
+    }
+    const float* zA = B.zA;
+    CF_ROWS(row, n)
+    {
+        const float t = row_f32<MW>(A, row, __fmul_rn(__ldg(B.diag + row), ld(zA + row)),
+                                    [&](int c) { return ld(zA + c); });
+        B.tA[row] = t;
+        acc[0] += (double)ld(B.sA + row) * (double)t;
+        acc[1] += (double)t * (double)t;
+    }
+    if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
+    {
+        st->tAsA = acc[0];
+        st->tAtA = acc[1];
+        st->omega = st->tAsA / st->tAtA;
+    }
+}
+
+__device__ __forceinline__ void p_bicg_e(const BicgBufs& B, volatile InnerState* st,
+                                         unsigned int* ticket, double* part)
+{
+    const int n = B.n;
+    const float alpha = (float)st->alpha;
+    const float omega = (float)st->omega;
+    const float* D = B.D + (size_t)st->cur * n;
+    float* Dn = B.D + (size_t)st->nxt * n;
+    double acc[2] = {0.0, 0.0};
+    CF_ROWS(row, n)
+    {
+        Dn[row] = __fadd_rn(ld(D + row), __fadd_rn(__fmul_rn(alpha, ld(B.yA + row)),
+                                                   __fmul_rn(omega, ld(B.zA + row))));
+        const float r = __fsub_rn(ld(B.sA + row), __fmul_rn(omega, ld(B.tA + row)));
+        B.rA[row] = r;
+        acc[0] += (double)fabsf(r);
+        acc[1] += (double)ld(B.rA0 + row) * (double)r;
+    }
+    if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
+    {
+        st->res = acc[0];
+        st->cur = st->nxt;
+        st->it = st->it + 1;
+        inner_sync_point(st, false);
+        st->rA0rAold = st->rA0rA;
+        st->rA0rA = acc[1];
+        st->beta = (st->rA0rA / st->rA0rAold) * (st->alpha / st->omega);
+    }
+}
+
+// launch_bicg_body's five phases (each skipped once the solve is done, as
+// the graph body's kernels return early), repeated until done
+__global__ void __launch_bounds__(NT) kp_bicg(DevSell A, BicgBufs B, InnerState* stp,
+                                              double* part, Bar bar)
+{
+    volatile InnerState* st = stp;
+    unsigned int* ticket = &stp->ticket;
+    while (!st->done)
+    {
+        p_bicg_a(B, st);
+        if (!grid_barrier(bar)) return;
+        p_bicg_b(A, B, st, ticket, part);
+        if (!grid_barrier(bar)) return;
+        p_bicg_c(B, st, ticket, part);
+        if (!grid_barrier(bar)) return;
+        if (!st->done || st->early) p_bicg_d(A, B, st, ticket, part);
+        if (!grid_barrier(bar)) return;
+        if (!st->done) p_bicg_e(B, st, ticket, part);
+        if (!grid_barrier(bar)) return;
+    }
+}
+
+}  // namespace
+
+namespace cf {
+
+int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran)
+{
+    *ran = false;
+    const int limit = maxCells == 0 ? (1 << 18) : maxCells;
+    if (limit < 0 || c->n > limit || !c->coopLaunch || !c->d_bar) return CF_OK;
+    const int n = c->n;
+    const int need = (n + NT - 1) / NT;
+    // the phase kernels of the graph path run on `need` blocks exactly
+    // when each one's resident capacity covers it; the persistent grid must
+    // be co-resident
+    const void* fn = kind == 0 ? (order > 1 ? (const void*)kp_pcg<true> : (const void*)kp_pcg<false>)
+                               : (const void*)kp_bicg;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, 0) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return CF_OK;
+    }
+    if ((long long)occ * c->numSMs < need) return CF_OK;
+    const void* phases[6];
+    int np = 0;
+    if (kind == 0)
+    {
+        phases[np++] = (const void*)k_cheb_step<true, MW>;
+        phases[np++] = (const void*)k_cheb_step<false, MW>;
+        phases[np++] = (const void*)k_pcg_p_spmv<MW>;
+        phases[np++] = order > 1 ? (const void*)k_pcg_update<true> : (const void*)k_pcg_update<false>;
+    }
+    else
+    {
+        phases[np++] = (const void*)k_bicg_a;
+        phases[np++] = (const void*)k_bicg_b<MW>;
+        phases[np++] = (const void*)k_bicg_c;
+        phases[np++] = (const void*)k_bicg_d<MW>;
+        phases[np++] = (const void*)k_bicg_e;
+    }
+    for (int i = 0; i < np; ++i)
+        if (grid_for(c, phases[i], n) != need) return CF_OK;
+
+    cudaStream_t s = c->stream;
+    if (cudaMemsetAsync(c->d_bar, 0, sizeof(unsigned int) * 4, s) != cudaSuccess)
+        return fail(CF_ERR_CUDA, "cudaMemsetAsync (grid barrier)");
+    const DevSell A = sell_of(c);
+    Bar bar{c->d_bar, c->d_bar + 1, reinterpret_cast<int*>(c->d_bar + 2)};
+    cudaError_t e;
+    if (kind == 0)
+    {
+        PcgBufs B = pcg_bufs(c);
+        InnerState* st = c->d_st;
+        double* part = c->d_part;
+        int ord = order;
+        void* args[] = {(void*)&A, (void*)&B, (void*)&ord, (void*)&st, (void*)&part, (void*)&bar};
+        e = cudaLaunchCooperativeKernel(fn, dim3(need), dim3(NT), args, 0, s);
+    }
+    else
+    {
+        BicgBufs B = bicg_bufs(c);
+        InnerState* st = c->d_st;
+        double* part = c->d_part;
+        void* args[] = {(void*)&A, (void*)&B, (void*)&st, (void*)&part, (void*)&bar};
+        e = cudaLaunchCooperativeKernel(fn, dim3(need), dim3(NT), args, 0, s);
+    }
+    if (e != cudaSuccess)
+        return fail(CF_ERR_CUDA, std::string("cudaLaunchCooperativeKernel: ") + cudaGetErrorString(e));
+    c->launches++;
+    *ran = true;
+    return CF_OK;
+}
+
+int persistent_status(cf_context* c)
+{
+    int err = 0;
+    if (cudaMemcpy(&err, c->d_bar + 2, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(CF_ERR_CUDA, "reading the grid-barrier status");
+    if (err) return fail(CF_ERR_DEVICE_TIMEOUT, "a grid barrier of the persistent inner solve timed out");
+    return CF_OK;
+}
+
+}  // namespace cf

@@ -222,7 +222,8 @@ int get_graph(cf_context* c, int kind, int order, cudaGraphExec_t* out, int* bod
 // the right-hand side; `mean` (device, may be NULL) is subtracted from it.
 // kind 0: PCG (metalFoamBackend::pcg), 1: BiCGStab (::bicgstab).
 int inner_solve(cf_context* c, int kind, const double* mean, double target, int maxIter, int ips,
-                int order, int useGraph, cf_inner_stats* stats, int stagLimit = STAG_LIMIT)
+                int order, int useGraph, cf_inner_stats* stats, int stagLimit = STAG_LIMIT,
+                int persistMax = 0)
 {
     const double tw0 = wall_now();
     cudaStream_t s = c->stream;
@@ -253,9 +254,17 @@ int inner_solve(cf_context* c, int kind, const double* mean, double target, int 
     }
     CF_LAUNCH();
     CF_CUDA(cudaEventRecord(c->ev0, s));
+    bool persistent = false;
     if (maxIter > 0)
     {
-        if (useGraph)
+        // small meshes: the whole loop as one cooperative kernel
+        if (useGraph && spmv_default(c))
+            CF_TRY(persistent_inner(c, kind, kind == 0 ? order : 1, persistMax, &persistent));
+        if (persistent)
+        {
+            c->pendingBodyKernels = 0;
+        }
+        else if (useGraph)
         {
             cudaGraphExec_t exec;
             int nk = 0;
@@ -291,6 +300,7 @@ int inner_solve(cf_context* c, int kind, const double* mean, double target, int 
     CF_LAUNCH();
     CF_CUDA(cudaMemcpyAsync(c->h_st, c->d_st, sizeof(InnerState), cudaMemcpyDeviceToHost, s));
     CF_CUDA(cudaStreamSynchronize(s));
+    if (persistent) CF_TRY(persistent_status(c));
     const InnerState& st = *c->h_st;
     if (c->pendingBodyKernels) c->launches += (long long)c->pendingBodyKernels * std::max(st.it, 1);
     float ms = 0.0f;
@@ -438,7 +448,8 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
             cf_inner_stats st;
             CF_TRY(inner_solve(c, bicg ? 1 : 0, meanp, target, o->maxIter - totalIter,
                                o->iterationsPerSync, order, o->graph, &st,
-                               o->stagnationLimit > 0 ? o->stagnationLimit : STAG_LIMIT));
+                               o->stagnationLimit > 0 ? o->stagnationLimit : STAG_LIMIT,
+                               o->persistentMaxCells));
             totalIter += st.nIterations;
             perf->tGpu += st.tGpuSeconds;
             perf->tInner += st.tWallSeconds;
