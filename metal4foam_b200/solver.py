@@ -143,7 +143,8 @@ def backend_cache_clear():
 
 
 _CONTROL_KEYS = ("maxRestarts", "iterationsPerSync", "deflate", "chebyshevOrder",
-                 "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit", "autotune")
+                 "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit", "autotune",
+                 "persistentMaxCells")
 
 # backends whose SpMV launch shape has been chosen (autotune yes)
 _TUNED: Dict[tuple, dict] = {}
@@ -206,6 +207,7 @@ class cudaFoamSolver:
             verbose=bool(s.get("verbose", False)),
             graph=bool(s.get("graph", True)),
             stagnationLimit=int(s.get("stagnationLimit", 0)),
+            persistentMaxCells=int(s.get("persistentMaxCells", 0)),
         )
 
     def solveImpl(self, psi: np.ndarray, source: np.ndarray, cmpt: int = 0) -> solverPerformance:
