@@ -97,11 +97,12 @@ typedef struct
     int32_t stagnationLimit;   /* inner iterations without a new minimum of
                                   sum|r| before the inner solve stops; 0
                                   (default) = 50, metalFoamBackend.C:606   */
-    int32_t persistentMaxCells;/* with graph = 1: meshes up to this many
-                                  cells run each inner solve as ONE
+    int32_t persistentMaxCells;/* with graph = 1 and > 0: meshes up to this
+                                  many cells run each inner solve as ONE
                                   cooperative kernel (grid barriers between
                                   the phases of an iteration, bit-identical
-                                  results); 0 (default) = 262144, < 0 =
+                                  results; slower than the graph loop on
+                                  B200, kept for comparison); 0 (default):
                                   never                                    */
 } cf_options;
 

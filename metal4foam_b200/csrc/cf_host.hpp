@@ -178,7 +178,7 @@ int launch_spmv32_v(cf_context* c, const float* diag, const float* x, const floa
                     double* out);
 
 // Inner solve as one cooperative kernel (cf_persist.cu) when the mesh has
-// at most maxCells cells (0: 262144, < 0: never) and the launch fits;
+// at most maxCells cells (<= 0: never) and the launch fits;
 // *ran tells whether it was launched.  persistent_status reads the grid
 // barrier's error word after the stream has completed.
 int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran);

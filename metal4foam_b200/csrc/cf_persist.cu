@@ -22,6 +22,12 @@
 // error word and leaves, the others leave at their next barrier, and the
 // host reports CF_ERR_DEVICE_TIMEOUT.  The launch is cooperative, so all
 // blocks are co-resident and the bound is never reached in normal runs.
+//
+// Opt-in (cf_options.persistentMaxCells > 0): measured on B200 it is 20-35%
+// slower than the graph-driven loop on 16k-64k-cell meshes (PCG and
+// BiCGStab), whether the loads bypass L1 or not and whatever the barrier's
+// polling interval -- a device-side graph launches the next kernel node
+// faster than a grid barrier completes.
 #include "cudafoam.h"
 #include "cf_host.hpp"
 
@@ -373,8 +379,7 @@ namespace cf {
 int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran)
 {
     *ran = false;
-    const int limit = maxCells == 0 ? (1 << 18) : maxCells;
-    if (limit < 0 || c->n > limit || !c->coopLaunch || !c->d_bar) return CF_OK;
+    if (maxCells <= 0 || c->n > maxCells || !c->coopLaunch || !c->d_bar) return CF_OK;
     const int n = c->n;
     const int need = (n + NT - 1) / NT;
     // the phase kernels of the graph path run on `need` blocks exactly
