@@ -104,6 +104,13 @@ typedef struct
                                   results; slower than the graph loop on
                                   B200, kept for comparison); 0 (default):
                                   never                                    */
+    int32_t clusterMaxCells;   /* cudaPCG with graph = 1: meshes up to this
+                                  many cells (at most 16384, one row per
+                                  thread) whose columns lie mostly in their
+                                  own CTA run each inner solve inside one
+                                  thread-block cluster of up to 16 CTAs,
+                                  the work vectors in distributed shared
+                                  memory; 0 (default) = 16384, < 0 = never */
 } cf_options;
 
 /* solverPerformance plus the reference's profile/verbose figures

@@ -47,6 +47,7 @@ class Options(C.Structure):
         ("profile", C.c_int32), ("verbose", C.c_int32), ("graph", C.c_int32),
         ("stagnationLimit", C.c_int32),
         ("persistentMaxCells", C.c_int32),
+        ("clusterMaxCells", C.c_int32),
     ]
 
 

@@ -649,6 +649,27 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
                                     cudaMemcpyHostToDevice, c->stream));
         }
     }
+    // locality of the cluster PCG's row split (cf_cluster.cu): the share of
+    // entries whose column belongs to another CTA
+    {
+        c->clusterShift = cluster_shift(n);
+        long long entries = 0, remote = 0;
+        for (int32_t sl = 0; sl < nslices; ++sl)
+        {
+            const int32_t b0 = sliceOff[sl];
+            const int32_t w = (sliceOff[sl + 1] - b0) / SLICE;
+            for (int32_t k = 0; k < w; ++k)
+                for (int32_t l = 0; l < SLICE; ++l)
+                {
+                    const int32_t cc = col[(size_t)b0 + SLICE * k + l];
+                    if (cc == -1) continue;
+                    ++entries;
+                    const int32_t row = sl * SLICE + l;
+                    if (((cc & 0x7fffffff) >> c->clusterShift) != (row >> c->clusterShift)) ++remote;
+                }
+        }
+        c->clusterRemote = entries ? (double)remote / (double)entries : 0.0;
+    }
     CF_CUDA(cudaMemsetAsync(c->d_D, 0, sizeof(float) * 3 * N, c->stream));
     CF_CUDA(cudaStreamSynchronize(c->stream));
     c->hasTopo = true;

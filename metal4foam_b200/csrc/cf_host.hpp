@@ -110,6 +110,8 @@ struct cf_context
     // (CF_LAYOUT_*), rows per warp, block size, multi-RHS tile
     int maxCtasPerSM = 32;
     bool coopLaunch = false;               // device supports cooperative launches
+    int clusterShift = 10;                 // log2(rows per CTA) of the cluster PCG for this mesh
+    double clusterRemote = 1.0;            // fraction of entries whose column lies in another CTA
     unsigned int* d_bar = nullptr;         // grid barrier of persistent inner solves: count, generation, error
     int cfgLayout = 0;
     int cfgRowsPerWarp = 32;
@@ -182,6 +184,13 @@ int launch_spmv32_v(cf_context* c, const float* diag, const float* x, const floa
 // *ran tells whether it was launched.  persistent_status reads the grid
 // barrier's error word after the stream has completed.
 int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran);
+// Inner PCG inside one thread-block cluster (cf_cluster.cu) for meshes of
+// at most min(maxCells, 16384) cells whose columns lie mostly in their own
+// CTA; *ran tells whether it was launched.
+int cluster_inner(cf_context* c, int order, int maxCells, bool* ran);
+// log2(rows per CTA) of the cluster PCG for an n-row mesh: the smallest
+// power of two >= 32 that needs at most 16 CTAs.
+int cluster_shift(int n);
 int persistent_status(cf_context* c);
 
 }  // namespace cf

@@ -223,7 +223,7 @@ int get_graph(cf_context* c, int kind, int order, cudaGraphExec_t* out, int* bod
 // kind 0: PCG (metalFoamBackend::pcg), 1: BiCGStab (::bicgstab).
 int inner_solve(cf_context* c, int kind, const double* mean, double target, int maxIter, int ips,
                 int order, int useGraph, cf_inner_stats* stats, int stagLimit = STAG_LIMIT,
-                int persistMax = 0)
+                int persistMax = 0, int clusterMax = 0)
 {
     const double tw0 = wall_now();
     cudaStream_t s = c->stream;
@@ -255,12 +255,16 @@ int inner_solve(cf_context* c, int kind, const double* mean, double target, int 
     CF_LAUNCH();
     CF_CUDA(cudaEventRecord(c->ev0, s));
     bool persistent = false;
+    bool clustered = false;
     if (maxIter > 0)
     {
-        // small meshes: the whole loop as one cooperative kernel
-        if (useGraph && spmv_default(c))
+        // small PCG systems: the whole loop inside one thread-block cluster
+        if (useGraph && spmv_default(c) && kind == 0 && clusterMax >= 0)
+            CF_TRY(cluster_inner(c, order, clusterMax == 0 ? 16384 : clusterMax, &clustered));
+        // opt-in: the whole loop as one cooperative kernel
+        if (!clustered && useGraph && spmv_default(c))
             CF_TRY(persistent_inner(c, kind, kind == 0 ? order : 1, persistMax, &persistent));
-        if (persistent)
+        if (persistent || clustered)
         {
             c->pendingBodyKernels = 0;
         }
@@ -449,7 +453,7 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
             CF_TRY(inner_solve(c, bicg ? 1 : 0, meanp, target, o->maxIter - totalIter,
                                o->iterationsPerSync, order, o->graph, &st,
                                o->stagnationLimit > 0 ? o->stagnationLimit : STAG_LIMIT,
-                               o->persistentMaxCells));
+                               o->persistentMaxCells, o->clusterMaxCells));
             totalIter += st.nIterations;
             perf->tGpu += st.tGpuSeconds;
             perf->tInner += st.tWallSeconds;

@@ -198,6 +198,7 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     opts.graph = cudaDict_.getOrDefault<bool>("graph", true);
     opts.stagnationLimit = cudaDict_.getOrDefault<label>("stagnationLimit", 0);
     opts.persistentMaxCells = cudaDict_.getOrDefault<label>("persistentMaxCells", 0);
+    opts.clusterMaxCells = cudaDict_.getOrDefault<label>("clusterMaxCells", 0);
 
     // autotune yes: time the SpMV launch shapes once per context (the mesh
     // of a context does not change during a run) and keep the fastest

@@ -144,7 +144,7 @@ def backend_cache_clear():
 
 _CONTROL_KEYS = ("maxRestarts", "iterationsPerSync", "deflate", "chebyshevOrder",
                  "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit", "autotune",
-                 "persistentMaxCells")
+                 "persistentMaxCells", "clusterMaxCells")
 
 # backends whose SpMV launch shape has been chosen (autotune yes)
 _TUNED: Dict[tuple, dict] = {}
@@ -208,6 +208,7 @@ class cudaFoamSolver:
             graph=bool(s.get("graph", True)),
             stagnationLimit=int(s.get("stagnationLimit", 0)),
             persistentMaxCells=int(s.get("persistentMaxCells", 0)),
+            clusterMaxCells=int(s.get("clusterMaxCells", 0)),
         )
 
     def solveImpl(self, psi: np.ndarray, source: np.ndarray, cmpt: int = 0) -> solverPerformance:

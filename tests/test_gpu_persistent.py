@@ -22,7 +22,7 @@ def run(s, solver, persistent, **kw):
     ctx.set_coeffs(s.diag, s.upper, s.lower)
     x = np.zeros(s.n)
     l0 = ctx.kernel_launches()
-    opts = dict(persistentMaxCells=1 << 20 if persistent else 0)
+    opts = dict(persistentMaxCells=1 << 20 if persistent else 0, clusterMaxCells=-1)
     opts.update(kw)
     p = ctx.solve(solver, x, s.source, _lib.default_options(**opts))
     launches = ctx.kernel_launches() - l0
