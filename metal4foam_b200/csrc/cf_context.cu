@@ -597,7 +597,7 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
     CF_TRY(dalloc(c, &c->d_Z0, N));
     CF_TRY(dalloc(c, &c->d_Z1, N));
     CF_TRY(dalloc(c, &c->d_P, 2 * N));
-    CF_TRY(dalloc(c, &c->d_Q, N));
+    CF_TRY(dalloc(c, &c->d_Q, 2 * N));   // PCG: q; BiCGStab: A yA ping-pong
     CF_TRY(dalloc(c, &c->d_T, N));
     CF_TRY(dalloc(c, &c->d_D, 3 * N));
     CF_TRY(dalloc(c, &c->d_io32, N));

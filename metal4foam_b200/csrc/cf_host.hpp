@@ -82,7 +82,7 @@ struct cf_context
     float* d_Z0 = nullptr;
     float* d_Z1 = nullptr;
     float* d_P = nullptr;                  // 2n
-    float* d_Q = nullptr;
+    float* d_Q = nullptr;                  // 2n (BiCGStab's A yA ping-pong)
     float* d_T = nullptr;
     float* d_D = nullptr;                  // 3n
     float* d_io32 = nullptr;
@@ -174,8 +174,8 @@ int stage_face32(cf_context* c, const double* up, const double* lo, int sym32);
 int launch_cheb_step_v(cf_context* c, bool last, const PcgBufs& B, const float* zin,
                        const float* win, float* wout, float* zout, int j);
 int launch_pcg_p_spmv_v(cf_context* c, const PcgBufs& B, const float* wA);
-int launch_bicg_b_v(cf_context* c, const BicgBufs& B);
-int launch_bicg_d_v(cf_context* c, const BicgBufs& B);
+int launch_bicg_ab_v(cf_context* c, const BicgBufs& B);
+int launch_bicg_cd_v(cf_context* c, const BicgBufs& B, cudaGraphConditionalHandle h, int useCond);
 int launch_spmv32_v(cf_context* c, const float* diag, const float* x, const float* w, float* y,
                     double* out);
 

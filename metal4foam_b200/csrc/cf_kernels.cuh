@@ -901,9 +901,9 @@ struct BicgBufs
 {
     float* rA;
     float* rA0;
-    float* P;
+    float* P;           // [2n] search direction ping-pong (by iteration parity)
     float* yA;
-    float* AyA;
+    float* AyA;         // [2n] A yA ping-pong (by iteration parity)
     float* sA;
     float* zA;
     float* tA;
@@ -915,7 +915,8 @@ struct BicgBufs
 };
 
 // Start of the inner BiCGStab (metalFoamBackend.C:761-770): rA, rA0 = rA,
-// delta = p = AyA = 0; then rA0.rA and reduce_scalars mode 3 (firstIter).
+// delta = p = AyA = 0 (both parities: iteration 0 reads the odd ones as
+// "previous"); then rA0.rA and reduce_scalars mode 3 (firstIter).
 static __global__ void __launch_bounds__(NT) k_bicg_init(BicgBufs B, const double* mean,
                                                   InnerState* st, double* part)
 {
@@ -929,7 +930,9 @@ static __global__ void __launch_bounds__(NT) k_bicg_init(BicgBufs B, const doubl
         B.rA0[row] = ra;
         B.D[row] = 0.0f;
         B.P[row] = 0.0f;
+        B.P[n + row] = 0.0f;
         B.AyA[row] = 0.0f;
+        B.AyA[n + row] = 0.0f;
         acc[0] += (double)ra * (double)ra;
     }
     if (grid_sum<1>(acc, part, &st->ticket) && threadIdx.x == 0)
@@ -940,36 +943,40 @@ static __global__ void __launch_bounds__(NT) k_bicg_init(BicgBufs B, const doubl
     }
 }
 
-// bicg_update_p + emul (metalFoamKernels.metal:198-208,372-386):
-// p = rA + beta (p - omega AyA); yA = rD p.
-static __global__ void __launch_bounds__(NT) k_bicg_a(BicgBufs B, InnerState* st)
+// bicg_update_p + emul (metalFoamKernels.metal:198-208,372-386) fused into
+// the SpMV ldu_spmv_dotw + reduce_scalars mode 4: p = rA + beta (p_old -
+// omega AyA_old) and yA = rD p are formed on the fly for every gathered
+// column (the previous iteration's p and AyA sit in the other parity), so
+// they need no pass of their own; writes p, yA, AyA = A yA for the own row;
+// rA0.AyA -> alpha.
+template <int MAXW>
+static __global__ void __launch_bounds__(NT) k_bicg_ab(DevSell A, BicgBufs B, InnerState* st,
+                                                double* part)
 {
     if (st->done) return;
+    const int n = A.n;
+    const int par = st->it & 1;
+    const float* __restrict__ Pold = B.P + (size_t)(par ^ 1) * n;
+    const float* __restrict__ Aold = B.AyA + (size_t)(par ^ 1) * n;
+    float* __restrict__ Pn = B.P + (size_t)par * n;
+    float* __restrict__ An = B.AyA + (size_t)par * n;
     const float beta = (float)st->beta;
     const float omega = (float)st->omega;
-    CF_ROWS(row, B.n)
-    {
-        const float p = __fadd_rn(B.rA[row],
-                                  __fmul_rn(beta, __fsub_rn(B.P[row], __fmul_rn(omega, B.AyA[row]))));
-        B.P[row] = p;
-        B.yA[row] = __fmul_rn(B.rD[row], p);
-    }
-}
-
-// AyA = A yA with rA0.AyA -> alpha (ldu_spmv_dotw + reduce_scalars mode 4).
-template <int MAXW>
-static __global__ void __launch_bounds__(NT) k_bicg_b(DevSell A, BicgBufs B, InnerState* st,
-                                               double* part)
-{
-    if (st->done) return;
-    const float* __restrict__ yA = B.yA;
+    auto pf = [&](int c) {
+        return __fadd_rn(__ldg(B.rA + c),
+                         __fmul_rn(beta, __fsub_rn(__ldg(Pold + c), __fmul_rn(omega, __ldg(Aold + c)))));
+    };
+    auto yf = [&](int c) { return __fmul_rn(__ldg(B.rD + c), pf(c)); };
     double acc[1] = {0.0};
-    CF_ROWS(row, A.n)
+    CF_ROWS(row, n)
     {
-        const float y = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], yA[row]),
-                                      [&](int c) { return __ldg(yA + c); });
-        B.AyA[row] = y;
-        acc[0] += (double)B.rA0[row] * (double)y;
+        const float p = pf(row);
+        const float y = __fmul_rn(B.rD[row], p);
+        Pn[row] = p;
+        B.yA[row] = y;
+        const float v = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], y), yf);
+        An[row] = v;
+        acc[0] += (double)B.rA0[row] * (double)v;
     }
     if (grid_sum<1>(acc, part, &st->ticket) && threadIdx.x == 0)
     {
@@ -978,23 +985,39 @@ static __global__ void __launch_bounds__(NT) k_bicg_b(DevSell A, BicgBufs B, Inn
     }
 }
 
-// bicg_s_res (metalFoamKernels.metal:390-412) + the zA = rD sA apply, then the
-// host checks of metalFoamBackend.C:829-866 on the device: breakdown on
-// rA0rA / alpha / sum|sA|, and the |sA| early exit.
-static __global__ void __launch_bounds__(NT) k_bicg_c(BicgBufs B, InnerState* st, double* part,
-                                               cudaGraphConditionalHandle h, int useCond)
+// bicg_s_res + emul (metalFoamKernels.metal:390-412) fused into the second
+// SpMV (reduce_scalars mode 5): s = rA - alpha AyA and zA = rD s are formed
+// on the fly for every gathered column; writes sA, zA, tA = A zA for the own
+// row; sum|s|, s.tA and tA.tA in one reduction.  The finaliser applies the
+// host checks of metalFoamBackend.C:829-866 first -- breakdown on rA0rA /
+// alpha / sum|s|, the |s| early exit -- and only then omega = s.tA / tA.tA.
+template <int MAXW>
+static __global__ void __launch_bounds__(NT) k_bicg_cd(DevSell A, BicgBufs B, InnerState* st,
+                                                double* part, cudaGraphConditionalHandle h,
+                                                int useCond)
 {
     if (st->done) return;
+    const int n = A.n;
+    const int par = st->it & 1;
+    const float* __restrict__ An = B.AyA + (size_t)par * n;
     const float alpha = (float)st->alpha;
-    double acc[1] = {0.0};
-    CF_ROWS(row, B.n)
+    auto zf = [&](int c) {
+        return __fmul_rn(__ldg(B.rD + c), __fsub_rn(__ldg(B.rA + c), __fmul_rn(alpha, __ldg(An + c))));
+    };
+    double acc[3] = {0.0, 0.0, 0.0};
+    CF_ROWS(row, n)
     {
-        const float sv = __fsub_rn(B.rA[row], __fmul_rn(alpha, B.AyA[row]));
+        const float sv = __fsub_rn(B.rA[row], __fmul_rn(alpha, An[row]));
+        const float z = __fmul_rn(B.rD[row], sv);
         B.sA[row] = sv;
-        B.zA[row] = __fmul_rn(B.rD[row], sv);
+        B.zA[row] = z;
         acc[0] += (double)fabsf(sv);
+        const float t = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], z), zf);
+        B.tA[row] = t;
+        acc[1] += (double)sv * (double)t;
+        acc[2] += (double)t * (double)t;
     }
-    if (grid_sum<1>(acc, part, &st->ticket) && threadIdx.x == 0)
+    if (grid_sum<3>(acc, part, &st->ticket) && threadIdx.x == 0)
     {
         st->resS = acc[0];
         if (!isfinite(st->rA0rA) || !isfinite(st->alpha) || !isfinite(st->resS))
@@ -1007,26 +1030,33 @@ static __global__ void __launch_bounds__(NT) k_bicg_c(BicgBufs B, InnerState* st
             st->early = 1;
             st->done = 1;
         }
+        else
+        {
+            st->tAsA = acc[1];
+            st->tAtA = acc[2];
+            st->omega = st->tAsA / st->tAtA;
+        }
         if (useCond && st->done) cudaGraphSetConditional(h, 0u);
     }
 }
 
-// Second SpMV: tA = A zA with sA.tA and tA.tA -> omega (reduce_scalars mode
-// 5); on the early-exit path instead delta += alpha yA (bicg_early_update).
-template <int MAXW>
-static __global__ void __launch_bounds__(NT) k_bicg_d(DevSell A, BicgBufs B, InnerState* st,
-                                               double* part)
+// bicg_update_sol_res (metalFoamKernels.metal:430-458) + the end-of-iteration
+// checks (metalFoamBackend.C:908-943) + the next iteration's rA0.rA and
+// beta (reduce_scalars mode 3).  On the |s| early exit instead delta +=
+// alpha yA (bicg_early_update) and the solve ends.
+static __global__ void __launch_bounds__(NT) k_bicg_e(BicgBufs B, InnerState* st, double* part,
+                                               cudaGraphConditionalHandle h, int useCond)
 {
     const bool early = st->early;
     if (st->done && !early) return;
-    const int n = A.n;
+    const int n = B.n;
+    const float alpha = (float)st->alpha;
+    const float* __restrict__ D = B.D + (size_t)st->cur * n;
+    float* __restrict__ Dn = B.D + (size_t)st->nxt * n;
     double acc[2] = {0.0, 0.0};
     if (early)
     {
         if (st->converged) return;   // already applied
-        const float alpha = (float)st->alpha;
-        const float* __restrict__ D = B.D + (size_t)st->cur * n;
-        float* __restrict__ Dn = B.D + (size_t)st->nxt * n;
         CF_ROWS(row, n) Dn[row] = __fadd_rn(D[row], __fmul_rn(alpha, B.yA[row]));
         if (grid_sum<2>(acc, part, &st->ticket) && threadIdx.x == 0)
         {
@@ -1037,36 +1067,7 @@ static __global__ void __launch_bounds__(NT) k_bicg_d(DevSell A, BicgBufs B, Inn
         }
         return;
     }
-    const float* __restrict__ zA = B.zA;
-    CF_ROWS(row, n)
-    {
-        const float t = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], zA[row]),
-                                      [&](int c) { return __ldg(zA + c); });
-        B.tA[row] = t;
-        acc[0] += (double)B.sA[row] * (double)t;
-        acc[1] += (double)t * (double)t;
-    }
-    if (grid_sum<2>(acc, part, &st->ticket) && threadIdx.x == 0)
-    {
-        st->tAsA = acc[0];
-        st->tAtA = acc[1];
-        st->omega = st->tAsA / st->tAtA;
-    }
-}
-
-// bicg_update_sol_res (metalFoamKernels.metal:430-458) + the end-of-iteration
-// checks (metalFoamBackend.C:908-943) + the next iteration's rA0.rA and
-// beta (reduce_scalars mode 3).
-static __global__ void __launch_bounds__(NT) k_bicg_e(BicgBufs B, InnerState* st, double* part,
-                                               cudaGraphConditionalHandle h, int useCond)
-{
-    if (st->done) return;
-    const int n = B.n;
-    const float alpha = (float)st->alpha;
     const float omega = (float)st->omega;
-    const float* __restrict__ D = B.D + (size_t)st->cur * n;
-    float* __restrict__ Dn = B.D + (size_t)st->nxt * n;
-    double acc[2] = {0.0, 0.0};
     CF_ROWS(row, n)
     {
         Dn[row] = __fadd_rn(D[row], __fadd_rn(__fmul_rn(alpha, B.yA[row]),

@@ -1,9 +1,9 @@
-// cf_persist.cu -- the inner PCG / BiCGStab loop of a small mesh as ONE
-// cooperative kernel.
+// cf_persist.cu -- the inner PCG loop of a small mesh as ONE cooperative
+// kernel.
 //
 // For meshes whose rows fit one per thread in a co-resident grid, the
-// phases of an iteration (Chebyshev steps, p-update SpMV, update; or the
-// five BiCGStab phases) run inside one launch separated by grid barriers,
+// phases of an iteration (Chebyshev steps, p-update SpMV, update) run
+// inside one launch separated by grid barriers,
 // and the launch loops until the device-side stopping tests end the inner
 // solve -- no kernel launch and no graph node per phase.  Each phase is the
 // arithmetic of the corresponding kernel of cf_kernels.cuh on the same
@@ -23,9 +23,10 @@
 // host reports CF_ERR_DEVICE_TIMEOUT.  The launch is cooperative, so all
 // blocks are co-resident and the bound is never reached in normal runs.
 //
-// Opt-in (cf_options.persistentMaxCells > 0): measured on B200 it is 20-35%
-// slower than the graph-driven loop on 16k-64k-cell meshes (PCG and
-// BiCGStab), whether the loads bypass L1 or not and whatever the barrier's
+// Opt-in (cf_options.persistentMaxCells > 0, cudaPCG): measured on B200 it
+// is 20-35% slower than the graph-driven loop on 16k-64k-cell meshes (PCG,
+// and BiCGStab before that loop was dropped from this file), whether the
+// loads bypass L1 or not and whatever the barrier's
 // polling interval -- a device-side graph launches the next kernel node
 // faster than a grid barrier completes.
 #include "cudafoam.h"
@@ -218,160 +219,6 @@ __global__ void __launch_bounds__(NT) kp_pcg(DevSell A, PcgBufs B, int order, In
     }
 }
 
-// ---------------------------------------------------------------- BiCGStab
-
-__device__ __forceinline__ void p_bicg_a(const BicgBufs& B, volatile InnerState* st)
-{
-    const float beta = (float)st->beta;
-    const float omega = (float)st->omega;
-    CF_ROWS(row, B.n)
-    {
-        const float p = __fadd_rn(ld(B.rA + row),
-                                  __fmul_rn(beta, __fsub_rn(ld(B.P + row), __fmul_rn(omega, ld(B.AyA + row)))));
-        B.P[row] = p;
-        B.yA[row] = __fmul_rn(__ldg(B.rD + row), p);
-    }
-}
-
-__device__ __forceinline__ void p_bicg_b(const DevSell& A, const BicgBufs& B,
-                                         volatile InnerState* st, unsigned int* ticket,
-                                         double* part)
-{
-    const float* yA = B.yA;
-    double acc[1] = {0.0};
-    CF_ROWS(row, A.n)
-    {
-        const float y = row_f32<MW>(A, row, __fmul_rn(__ldg(B.diag + row), ld(yA + row)),
-                                    [&](int c) { return ld(yA + c); });
-        B.AyA[row] = y;
-        acc[0] += (double)ld(B.rA0 + row) * (double)y;
-    }
-    if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0)
-    {
-        st->rA0AyA = acc[0];
-        st->alpha = st->rA0rA / st->rA0AyA;
-    }
-}
-
-__device__ __forceinline__ void p_bicg_c(const BicgBufs& B, volatile InnerState* st,
-                                         unsigned int* ticket, double* part)
-{
-    const float alpha = (float)st->alpha;
-    double acc[1] = {0.0};
-    CF_ROWS(row, B.n)
-    {
-        const float sv = __fsub_rn(ld(B.rA + row), __fmul_rn(alpha, ld(B.AyA + row)));
-        B.sA[row] = sv;
-        B.zA[row] = __fmul_rn(__ldg(B.rD + row), sv);
-        acc[0] += (double)fabsf(sv);
-    }
-    if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0)
-    {
-        st->resS = acc[0];
-        if (!isfinite(st->rA0rA) || !isfinite(st->alpha) || !isfinite(st->resS))
-        {
-            st->singular = 1;
-            st->done = 1;
-        }
-        else if (st->resS <= st->target)
-        {
-            st->early = 1;
-            st->done = 1;
-        }
-    }
-}
-
-__device__ __forceinline__ void p_bicg_d(const DevSell& A, const BicgBufs& B,
-                                         volatile InnerState* st, unsigned int* ticket,
-                                         double* part)
-{
-    const int n = A.n;
-    double acc[2] = {0.0, 0.0};
-    if (st->early)
-    {
-        if (st->converged) return;
-        const float alpha = (float)st->alpha;
-        const float* D = B.D + (size_t)st->cur * n;
-        float* Dn = B.D + (size_t)st->nxt * n;
-        CF_ROWS(row, n) Dn[row] = __fadd_rn(ld(D + row), __fmul_rn(alpha, ld(B.yA + row)));
-        if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
-        {
-            st->cur = st->nxt;
-            st->it = st->it + 1;
-            st->finalResSum = st->resS;
-            st->converged = 1;
-        }
-        return;
-    }
-    const float* zA = B.zA;
-    CF_ROWS(row, n)
-    {
-        const float t = row_f32<MW>(A, row, __fmul_rn(__ldg(B.diag + row), ld(zA + row)),
-                                    [&](int c) { return ld(zA + c); });
-        B.tA[row] = t;
-        acc[0] += (double)ld(B.sA + row) * (double)t;
-        acc[1] += (double)t * (double)t;
-    }
-    if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
-    {
-        st->tAsA = acc[0];
-        st->tAtA = acc[1];
-        st->omega = st->tAsA / st->tAtA;
-    }
-}
-
-__device__ __forceinline__ void p_bicg_e(const BicgBufs& B, volatile InnerState* st,
-                                         unsigned int* ticket, double* part)
-{
-    const int n = B.n;
-    const float alpha = (float)st->alpha;
-    const float omega = (float)st->omega;
-    const float* D = B.D + (size_t)st->cur * n;
-    float* Dn = B.D + (size_t)st->nxt * n;
-    double acc[2] = {0.0, 0.0};
-    CF_ROWS(row, n)
-    {
-        Dn[row] = __fadd_rn(ld(D + row), __fadd_rn(__fmul_rn(alpha, ld(B.yA + row)),
-                                                   __fmul_rn(omega, ld(B.zA + row))));
-        const float r = __fsub_rn(ld(B.sA + row), __fmul_rn(omega, ld(B.tA + row)));
-        B.rA[row] = r;
-        acc[0] += (double)fabsf(r);
-        acc[1] += (double)ld(B.rA0 + row) * (double)r;
-    }
-    if (grid_sum<2>(acc, part, ticket) && threadIdx.x == 0)
-    {
-        st->res = acc[0];
-        st->cur = st->nxt;
-        st->it = st->it + 1;
-        inner_sync_point(st, false);
-        st->rA0rAold = st->rA0rA;
-        st->rA0rA = acc[1];
-        st->beta = (st->rA0rA / st->rA0rAold) * (st->alpha / st->omega);
-    }
-}
-
-// launch_bicg_body's five phases (each skipped once the solve is done, as
-// the graph body's kernels return early), repeated until done
-__global__ void __launch_bounds__(NT) kp_bicg(DevSell A, BicgBufs B, InnerState* stp,
-                                              double* part, Bar bar)
-{
-    volatile InnerState* st = stp;
-    unsigned int* ticket = &stp->ticket;
-    while (!st->done)
-    {
-        p_bicg_a(B, st);
-        if (!grid_barrier(bar)) return;
-        p_bicg_b(A, B, st, ticket, part);
-        if (!grid_barrier(bar)) return;
-        p_bicg_c(B, st, ticket, part);
-        if (!grid_barrier(bar)) return;
-        if (!st->done || st->early) p_bicg_d(A, B, st, ticket, part);
-        if (!grid_barrier(bar)) return;
-        if (!st->done) p_bicg_e(B, st, ticket, part);
-        if (!grid_barrier(bar)) return;
-    }
-}
-
 }  // namespace
 
 namespace cf {
@@ -379,14 +226,14 @@ namespace cf {
 int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran)
 {
     *ran = false;
-    if (maxCells <= 0 || c->n > maxCells || !c->coopLaunch || !c->d_bar) return CF_OK;
+    if (kind != 0 || maxCells <= 0 || c->n > maxCells || !c->coopLaunch || !c->d_bar)
+        return CF_OK;
     const int n = c->n;
     const int need = (n + NT - 1) / NT;
     // the phase kernels of the graph path run on `need` blocks exactly
     // when each one's resident capacity covers it; the persistent grid must
     // be co-resident
-    const void* fn = kind == 0 ? (order > 1 ? (const void*)kp_pcg<true> : (const void*)kp_pcg<false>)
-                               : (const void*)kp_bicg;
+    const void* fn = order > 1 ? (const void*)kp_pcg<true> : (const void*)kp_pcg<false>;
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, 0) != cudaSuccess)
     {
@@ -394,23 +241,11 @@ int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran
         return CF_OK;
     }
     if ((long long)occ * c->numSMs < need) return CF_OK;
-    const void* phases[6];
-    int np = 0;
-    if (kind == 0)
-    {
-        phases[np++] = (const void*)k_cheb_step<true, MW>;
-        phases[np++] = (const void*)k_cheb_step<false, MW>;
-        phases[np++] = (const void*)k_pcg_p_spmv<MW>;
-        phases[np++] = order > 1 ? (const void*)k_pcg_update<true> : (const void*)k_pcg_update<false>;
-    }
-    else
-    {
-        phases[np++] = (const void*)k_bicg_a;
-        phases[np++] = (const void*)k_bicg_b<MW>;
-        phases[np++] = (const void*)k_bicg_c;
-        phases[np++] = (const void*)k_bicg_d<MW>;
-        phases[np++] = (const void*)k_bicg_e;
-    }
+    const void* phases[4] = {(const void*)k_cheb_step<true, MW>, (const void*)k_cheb_step<false, MW>,
+                             (const void*)k_pcg_p_spmv<MW>,
+                             order > 1 ? (const void*)k_pcg_update<true>
+                                       : (const void*)k_pcg_update<false>};
+    const int np = 4;
     for (int i = 0; i < np; ++i)
         if (grid_for(c, phases[i], n) != need) return CF_OK;
 
@@ -419,24 +254,12 @@ int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran
         return fail(CF_ERR_CUDA, "cudaMemsetAsync (grid barrier)");
     const DevSell A = sell_of(c);
     Bar bar{c->d_bar, c->d_bar + 1, reinterpret_cast<int*>(c->d_bar + 2)};
-    cudaError_t e;
-    if (kind == 0)
-    {
-        PcgBufs B = pcg_bufs(c);
-        InnerState* st = c->d_st;
-        double* part = c->d_part;
-        int ord = order;
-        void* args[] = {(void*)&A, (void*)&B, (void*)&ord, (void*)&st, (void*)&part, (void*)&bar};
-        e = cudaLaunchCooperativeKernel(fn, dim3(need), dim3(NT), args, 0, s);
-    }
-    else
-    {
-        BicgBufs B = bicg_bufs(c);
-        InnerState* st = c->d_st;
-        double* part = c->d_part;
-        void* args[] = {(void*)&A, (void*)&B, (void*)&st, (void*)&part, (void*)&bar};
-        e = cudaLaunchCooperativeKernel(fn, dim3(need), dim3(NT), args, 0, s);
-    }
+    PcgBufs B = pcg_bufs(c);
+    InnerState* st = c->d_st;
+    double* part = c->d_part;
+    int ord = order;
+    void* args[] = {(void*)&A, (void*)&B, (void*)&ord, (void*)&st, (void*)&part, (void*)&bar};
+    const cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(need), dim3(NT), args, 0, s);
     if (e != cudaSuccess)
         return fail(CF_ERR_CUDA, std::string("cudaLaunchCooperativeKernel: ") + cudaGetErrorString(e));
     c->launches++;

@@ -115,35 +115,25 @@ int launch_bicg_body(cf_context* c, cudaGraphConditionalHandle h, int useCond, i
     const DevSell A = sell_of(c);
     const BicgBufs B = bicg_bufs(c);
     cudaStream_t s = c->stream;
-    k_bicg_a<<<grid_for(c, (const void*)k_bicg_a, c->n), NT, 0, s>>>(B, c->d_st);
-    CF_LAUNCH();
     if (!spmv_default(c))
     {
-        CF_TRY(launch_bicg_b_v(c, B));
+        CF_TRY(launch_bicg_ab_v(c, B));
+        CF_TRY(launch_bicg_cd_v(c, B, h, useCond));
     }
     else
     {
-        auto fn = k_bicg_b<MW>;
-        fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
+        auto fab = k_bicg_ab<MW>;
+        fab<<<grid_for(c, (const void*)fab, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
         CF_LAUNCH();
-    }
-    k_bicg_c<<<grid_for(c, (const void*)k_bicg_c, c->n), NT, 0, s>>>(B, c->d_st, c->d_part, h,
-                                                                    useCond);
-    CF_LAUNCH();
-    if (!spmv_default(c))
-    {
-        CF_TRY(launch_bicg_d_v(c, B));
-    }
-    else
-    {
-        auto fn = k_bicg_d<MW>;
-        fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
+        auto fcd = k_bicg_cd<MW>;
+        fcd<<<grid_for(c, (const void*)fcd, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part, h,
+                                                              useCond);
         CF_LAUNCH();
     }
     k_bicg_e<<<grid_for(c, (const void*)k_bicg_e, c->n), NT, 0, s>>>(B, c->d_st, c->d_part, h,
                                                                     useCond);
     CF_LAUNCH();
-    if (kernels) *kernels = 5;
+    if (kernels) *kernels = 3;
     return CF_OK;
 }
 
@@ -157,7 +147,7 @@ int get_graph(cf_context* c, int kind, int order, cudaGraphExec_t* out, int* bod
     if (it != c->graphs.end())
     {
         *out = it->second;
-        *bodyKernels = kind == 0 ? (order > 1 ? order + 1 : 2) : 5;
+        *bodyKernels = kind == 0 ? (order > 1 ? order + 1 : 2) : 3;
         return CF_OK;
     }
     cudaGraph_t g = nullptr;

@@ -307,24 +307,39 @@ __global__ void __launch_bounds__(BS) kt_pcg_p_spmv(Op op, int n, PcgBufs B, con
     }
 }
 
-// k_bicg_b in any launch shape
+// k_bicg_ab in any launch shape
 template <class Op, int G, int BS>
-__global__ void __launch_bounds__(BS) kt_bicg_b(Op op, int n, BicgBufs B, InnerState* st,
-                                                double* part)
+__global__ void __launch_bounds__(BS) kt_bicg_ab(Op op, int n, BicgBufs B, InnerState* st,
+                                                 double* part)
 {
     if (st->done) return;
     const int lane = threadIdx.x & (G - 1);
-    const float* __restrict__ yA = B.yA;
+    const int par = st->it & 1;
+    const float* __restrict__ Pold = B.P + (size_t)(par ^ 1) * n;
+    const float* __restrict__ Aold = B.AyA + (size_t)(par ^ 1) * n;
+    float* __restrict__ Pn = B.P + (size_t)par * n;
+    float* __restrict__ An = B.AyA + (size_t)par * n;
+    const float beta = (float)st->beta;
+    const float omega = (float)st->omega;
+    auto pf = [&](int c) {
+        return __fadd_rn(__ldg(B.rA + c),
+                         __fmul_rn(beta, __fsub_rn(__ldg(Pold + c), __fmul_rn(omega, __ldg(Aold + c)))));
+    };
+    auto yf = [&](int c) { return __fmul_rn(__ldg(B.rD + c), pf(c)); };
     double acc[1] = {0.0};
     CFT_ROWS(row, valid, n)
     {
         if (G == 1 && !valid) continue;
-        float y = valid ? __fmul_rn(B.diag[row], yA[row]) : 0.0f;
-        y = op_row<G>(op, row, valid, y, [&](int c) { return __ldg(yA + c); }, lane);
+        const float p = valid ? pf(row) : 0.0f;
+        const float y = valid ? __fmul_rn(B.rD[row], p) : 0.0f;
+        float v = valid ? __fmul_rn(B.diag[row], y) : 0.0f;
+        v = op_row<G>(op, row, valid, v, yf, lane);
         if (valid && lane == 0)
         {
-            B.AyA[row] = y;
-            acc[0] += (double)B.rA0[row] * (double)y;
+            Pn[row] = p;
+            B.yA[row] = y;
+            An[row] = v;
+            acc[0] += (double)B.rA0[row] * (double)v;
         }
     }
     if (grid_sum_bs<1, BS>(acc, part, &st->ticket) && threadIdx.x == 0)
@@ -334,50 +349,58 @@ __global__ void __launch_bounds__(BS) kt_bicg_b(Op op, int n, BicgBufs B, InnerS
     }
 }
 
-// k_bicg_d in any launch shape
+// k_bicg_cd in any launch shape
 template <class Op, int G, int BS>
-__global__ void __launch_bounds__(BS) kt_bicg_d(Op op, int n, BicgBufs B, InnerState* st,
-                                                double* part)
+__global__ void __launch_bounds__(BS) kt_bicg_cd(Op op, int n, BicgBufs B, InnerState* st,
+                                                 double* part, cudaGraphConditionalHandle h,
+                                                 int useCond)
 {
-    const bool early = st->early;
-    if (st->done && !early) return;
+    if (st->done) return;
     const int lane = threadIdx.x & (G - 1);
-    double acc[2] = {0.0, 0.0};
-    if (early)
-    {
-        if (st->converged) return;   // already applied
-        const float alpha = (float)st->alpha;
-        const float* __restrict__ D = B.D + (size_t)st->cur * n;
-        float* __restrict__ Dn = B.D + (size_t)st->nxt * n;
-        for (int row = blockIdx.x * BS + threadIdx.x; row < n; row += gridDim.x * BS)
-            Dn[row] = __fadd_rn(D[row], __fmul_rn(alpha, B.yA[row]));
-        if (grid_sum_bs<2, BS>(acc, part, &st->ticket) && threadIdx.x == 0)
-        {
-            st->cur = st->nxt;
-            st->it = st->it + 1;
-            st->finalResSum = st->resS;
-            st->converged = 1;
-        }
-        return;
-    }
-    const float* __restrict__ zA = B.zA;
+    const int par = st->it & 1;
+    const float* __restrict__ An = B.AyA + (size_t)par * n;
+    const float alpha = (float)st->alpha;
+    auto zf = [&](int c) {
+        return __fmul_rn(__ldg(B.rD + c), __fsub_rn(__ldg(B.rA + c), __fmul_rn(alpha, __ldg(An + c))));
+    };
+    double acc[3] = {0.0, 0.0, 0.0};
     CFT_ROWS(row, valid, n)
     {
         if (G == 1 && !valid) continue;
-        float t = valid ? __fmul_rn(B.diag[row], zA[row]) : 0.0f;
-        t = op_row<G>(op, row, valid, t, [&](int c) { return __ldg(zA + c); }, lane);
+        const float sv = valid ? __fsub_rn(B.rA[row], __fmul_rn(alpha, An[row])) : 0.0f;
+        const float z = valid ? __fmul_rn(B.rD[row], sv) : 0.0f;
+        float t = valid ? __fmul_rn(B.diag[row], z) : 0.0f;
+        t = op_row<G>(op, row, valid, t, zf, lane);
         if (valid && lane == 0)
         {
+            B.sA[row] = sv;
+            B.zA[row] = z;
             B.tA[row] = t;
-            acc[0] += (double)B.sA[row] * (double)t;
-            acc[1] += (double)t * (double)t;
+            acc[0] += (double)fabsf(sv);
+            acc[1] += (double)sv * (double)t;
+            acc[2] += (double)t * (double)t;
         }
     }
-    if (grid_sum_bs<2, BS>(acc, part, &st->ticket) && threadIdx.x == 0)
+    if (grid_sum_bs<3, BS>(acc, part, &st->ticket) && threadIdx.x == 0)
     {
-        st->tAsA = acc[0];
-        st->tAtA = acc[1];
-        st->omega = st->tAsA / st->tAtA;
+        st->resS = acc[0];
+        if (!isfinite(st->rA0rA) || !isfinite(st->alpha) || !isfinite(st->resS))
+        {
+            st->singular = 1;
+            st->done = 1;
+        }
+        else if (st->resS <= st->target)
+        {
+            st->early = 1;
+            st->done = 1;
+        }
+        else
+        {
+            st->tAsA = acc[1];
+            st->tAtA = acc[2];
+            st->omega = st->tAsA / st->tAtA;
+        }
+        if (useCond && st->done) cudaGraphSetConditional(h, 0u);
     }
 }
 
@@ -670,28 +693,28 @@ int launch_pcg_p_spmv_v(cf_context* c, const PcgBufs& B, const float* wA)
     });
 }
 
-int launch_bicg_b_v(cf_context* c, const BicgBufs& B)
+int launch_bicg_ab_v(cf_context* c, const BicgBufs& B)
 {
     return dispatch(c, [&](const auto& op, auto g, auto b) -> int {
         using Op = std::decay_t<decltype(op)>;
         constexpr int G = decltype(g)::value;
         constexpr int BS = decltype(b)::value;
-        auto fn = kt_bicg_b<Op, G, BS>;
+        auto fn = kt_bicg_ab<Op, G, BS>;
         fn<<<grid_v(c, (const void*)fn, c->n, G, BS), BS, 0, c->stream>>>(op, c->n, B, c->d_st,
                                                                            c->d_part);
         return launched(c);
     });
 }
 
-int launch_bicg_d_v(cf_context* c, const BicgBufs& B)
+int launch_bicg_cd_v(cf_context* c, const BicgBufs& B, cudaGraphConditionalHandle h, int useCond)
 {
     return dispatch(c, [&](const auto& op, auto g, auto b) -> int {
         using Op = std::decay_t<decltype(op)>;
         constexpr int G = decltype(g)::value;
         constexpr int BS = decltype(b)::value;
-        auto fn = kt_bicg_d<Op, G, BS>;
+        auto fn = kt_bicg_cd<Op, G, BS>;
         fn<<<grid_v(c, (const void*)fn, c->n, G, BS), BS, 0, c->stream>>>(op, c->n, B, c->d_st,
-                                                                           c->d_part);
+                                                                           c->d_part, h, useCond);
         return launched(c);
     });
 }

@@ -1,5 +1,5 @@
-"""Persistent inner solves (opt-in, persistentMaxCells > 0): on small
-meshes the whole inner loop runs as one cooperative kernel with grid
+"""Persistent inner solves (opt-in, persistentMaxCells > 0, cudaPCG): on
+small meshes the whole inner loop runs as one cooperative kernel with grid
 barriers between the phases.  It must return exactly what the graph-driven
 loop returns (same grid, same reductions): psi bit for bit, the same
 iterations, restarts and residuals -- and launch far fewer kernels."""
@@ -41,10 +41,6 @@ CASES = [
      _lib.CF_SOLVER_PCG, dict(chebyshevOrder=1, deflate="off", maxIter=3000)),
     ("varcoeff_ips4", lambda: mesh.varcoeff3d((20, 20, 20), seed=6, permute=True),
      _lib.CF_SOLVER_PCG, dict(iterationsPerSync=4, tolerance=1e-8)),
-    ("upwind_30", lambda: mesh.upwind3d((30, 30, 30), seed=7), _lib.CF_SOLVER_PBICGSTAB,
-     dict(tolerance=1e-8, maxIter=3000)),
-    ("upwind_early", lambda: mesh.upwind3d((12, 10, 8), seed=8), _lib.CF_SOLVER_PBICGSTAB,
-     dict(tolerance=1e-3)),
 ]
 
 
