@@ -714,11 +714,7 @@ static __global__ void __launch_bounds__(NT) k_pcg_init(PcgBufs B, const double*
 // encoded per step at metalFoamBackend.C:365-384) fused into one pass:
 //   v = A z_{j-1};  w = c2 w + c3 rD (r - v);  z_j = z_{j-1} + w.
 // On the last step the z.r dot and reduce_scalars mode 0 (wArA, beta) follow.
-// RW rows per thread (rows r, r + NT, ... of a block's RW * NT-row step):
-// with RW = 2 both rows' column and value loads are in flight before either
-// row's gathers, which a latency-bound SpMV turns into bandwidth (used when
-// the grid is capped at the resident capacity, i.e. on large meshes).
-template <bool LAST, int MAXW, int RW = 1>
+template <bool LAST, int MAXW>
 static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
                                                   const float* win, float* wout, float* zout,
                                                   int j, InnerState* st, double* part)
@@ -727,31 +723,18 @@ static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, c
     const float c2 = B.chebC[2 * j - 1];
     const float c3 = B.chebC[2 * j];
     double acc[1] = {0.0};
-    for (int r0 = blockIdx.x * RW * NT + threadIdx.x; r0 < A.n; r0 += gridDim.x * RW * NT)
+    CF_ROWS(row, A.n)
     {
-        float zr[RW], v[RW];
-#pragma unroll
-        for (int k = 0; k < RW; ++k)
-        {
-            const int row = r0 + k * NT;
-            zr[k] = row < A.n ? zin[row] : 0.0f;
-            v[k] = row < A.n ? row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], zr[k]),
-                                             [&](int c) { return __ldg(zin + c); })
-                             : 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < RW; ++k)
-        {
-            const int row = r0 + k * NT;
-            if (row >= A.n) break;
-            const float r = B.rA[row];
-            const float wn = __fadd_rn(__fmul_rn(c2, win[row]),
-                                       __fmul_rn(__fmul_rn(c3, B.rD[row]), __fsub_rn(r, v[k])));
-            const float zn = __fadd_rn(zr[k], wn);
-            wout[row] = wn;
-            zout[row] = zn;
-            if (LAST) acc[0] += (double)zn * (double)r;
-        }
+        const float zr = zin[row];
+        const float v = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], zr),
+                                      [&](int c) { return __ldg(zin + c); });
+        const float r = B.rA[row];
+        const float wn = __fadd_rn(__fmul_rn(c2, win[row]),
+                                   __fmul_rn(__fmul_rn(c3, B.rD[row]), __fsub_rn(r, v)));
+        const float zn = __fadd_rn(zr, wn);
+        wout[row] = wn;
+        zout[row] = zn;
+        if (LAST) acc[0] += (double)zn * (double)r;
     }
     if (LAST)
     {

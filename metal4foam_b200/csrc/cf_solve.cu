@@ -41,31 +41,6 @@ constexpr int MW = MAXW_UNROLL;
 
 int chebz(int j) { return j & 1; }
 
-// One Chebyshev step in the default shape: one row per thread while the
-// grid covers every row at once, two rows per thread on meshes that exceed
-// the resident capacity (measured 23.6 -> 22.7 us per step at 128^3; three
-// or four rows per thread were slower).
-template <bool LAST>
-int cheb_step_default(cf_context* c, const DevSell& A, const PcgBufs& B, const float* zin,
-                      const float* win, float* wout, float* zout, int j)
-{
-    const int n = c->n;
-    auto f1 = k_cheb_step<LAST, MW, 1>;
-    const int g1 = grid_for(c, (const void*)f1, n);
-    if ((long long)g1 * NT >= n)
-    {
-        f1<<<g1, NT, 0, c->stream>>>(A, B, zin, win, wout, zout, j, c->d_st, c->d_part);
-    }
-    else
-    {
-        auto f2 = k_cheb_step<LAST, MW, 2>;
-        f2<<<grid_for(c, (const void*)f2, (n + 1) / 2), NT, 0, c->stream>>>(
-            A, B, zin, win, wout, zout, j, c->d_st, c->d_part);
-    }
-    CF_LAUNCH();
-    return CF_OK;
-}
-
 // One PCG iteration (Chebyshev steps, p-update+SpMV, update); identical
 // for graph capture and for host-synchronised execution.
 int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int useCond,
@@ -91,9 +66,18 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
                 continue;
             }
             if (j == order - 1)
-                CF_TRY(cheb_step_default<true>(c, A, B, zin, win, B.W1, zout, j));
+            {
+                auto fn = k_cheb_step<true, MW>;
+                fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j,
+                                                                    c->d_st, c->d_part);
+            }
             else
-                CF_TRY(cheb_step_default<false>(c, A, B, zin, win, B.W1, zout, j));
+            {
+                auto fn = k_cheb_step<false, MW>;
+                fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j,
+                                                                    c->d_st, c->d_part);
+            }
+            CF_LAUNCH();
             ++nk;
         }
         wA = Z[chebz(order - 1)];
@@ -745,7 +729,10 @@ extern "C" int cf_cheb_apply(cf_context* c, const float* r, float* z, int32_t or
         }
         else
         {
-            CF_TRY(cheb_step_default<false>(c, A, B, zin, win, B.W1, Z[chebz(j)], j));
+            auto fn = k_cheb_step<false, MW>;
+            fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)],
+                                                             j, c->d_st, c->d_part);
+            CF_LAUNCH();
         }
         out = Z[chebz(j)];
     }
@@ -787,7 +774,10 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             {
                 if (!spmv_default(c))
                     return launch_cheb_step_v(c, false, B, B.Z0, B.W1, B.W1, B.Z1, 2);
-                return cheb_step_default<false>(c, A, B, B.Z0, B.W1, B.W1, B.Z1, 2);
+                auto fn = k_cheb_step<false, MW>;
+                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2,
+                                                                 c->d_st, c->d_part);
+                break;
             }
             case CF_KERNEL_SPMV32:
             {
