@@ -618,7 +618,11 @@ def run_ours(args, ws, rank, local):
     # error against an FP64 solve of the same system is checked in the tests;
     # here the FP64 residual of every timed solve is asserted
     # dominant kernel: the fused SpMV + Chebyshev step
-    t_cheb = ctx.time_kernel("cheb_step", reps=100)
+    # the Chebyshev step as it runs inside PCG iterations (cache state of a
+    # real solve); the same kernel repeated on unchanged buffers reads part
+    # of its 122 MB from L2 and is reported beside it
+    t_cheb = ctx.time_kernel("cheb_step_inner", reps=20)
+    t_cheb_rep = ctx.time_kernel("cheb_step", reps=100)
     t_spmv = ctx.time_kernel("spmv32", reps=100)
     t_amul = ctx.time_kernel("amul64", reps=20)
     peak, peak_kind = read_peaks()
@@ -683,7 +687,10 @@ def run_ours(args, ws, rank, local):
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": bytes_cheb,
-                         "ms_per_launch": round(t_cheb, 5)},
+                         "ms_per_launch": round(t_cheb, 5),
+                         "timing": "average of the 7 Chebyshev steps of 20 PCG iterations, "
+                                   "each bracketed by CUDA events on the solve stream",
+                         "ms_per_launch_repeated_kernel": round(t_cheb_rep, 5)},
             "spmv": {"kernel": "k_spmv32 (FP32 LDU SpMV + dot)",
                      "gbs": round(b_spmv(n, nf) / (t_spmv * 1e-3) / 1e9, 1),
                      "frac": round(b_spmv(n, nf) / (t_spmv * 1e-3) / 1e9 / peak, 4),

@@ -361,7 +361,8 @@ class Context:
         check(load().cf_spmv32(self.h, ptr(xx), ptr(ww), ptr(y), C.byref(d)))
         return y, d.value
 
-    KERNELS = {"cheb_step": 0, "spmv32": 1, "pcg_p_spmv": 2, "pcg_update": 3, "amul64": 4}
+    KERNELS = {"cheb_step": 0, "spmv32": 1, "pcg_p_spmv": 2, "pcg_update": 3, "amul64": 4,
+               "cheb_step_inner": 5}
 
     def time_kernel(self, which, reps=50):
         ms = C.c_double()

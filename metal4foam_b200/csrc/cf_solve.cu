@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 using namespace cf;
 
@@ -767,6 +768,74 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
     k_cheb_init<<<g1, NT, 0, s>>>(n, B.rA, B.rD, c->d_chebC, B.W1);
     CF_LAUNCH();
     CF_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(float) * 2 * (size_t)n, s));
+    if (which == CF_KERNEL_CHEB_STEP_INNER)
+    {
+        // full PCG iterations (Chebyshev 8, p-update SpMV, update) launched
+        // one by one from the solve's own inner right-hand side, the 7 steps
+        // of each iteration bracketed by events
+        k_inner_setup<<<1, 32, 0, s>>>(c->d_st, 0.0, 1 << 30, 1, 1 << 30);
+        CF_LAUNCH();
+        k_pcg_init<true><<<grid_for(c, (const void*)k_pcg_init<true>, n), NT, 0, s>>>(
+            B, nullptr, c->d_st, c->d_part);
+        CF_LAUNCH();
+        const int steps = 7 * reps;
+        std::vector<cudaEvent_t> ev(2 * (size_t)steps, nullptr);
+        for (auto& e : ev)
+            if (cudaEventCreate(&e) != cudaSuccess)
+            {
+                for (auto& f : ev)
+                    if (f) cudaEventDestroy(f);
+                return fail(CF_ERR_CUDA, "cudaEventCreate");
+            }
+        int k = 0;
+        int rc = CF_OK;
+        float* Z[2] = {B.Z0, B.Z1};
+        for (int it = 0; it < reps && rc == CF_OK; ++it)
+        {
+            for (int j = 1; j < 8 && rc == CF_OK; ++j)
+            {
+                const float* zin = (j == 1) ? B.W0 : Z[chebz(j - 1)];
+                const float* win = (j == 1) ? B.W0 : B.W1;
+                cudaEventRecord(ev[2 * k], s);
+                if (j == 7)
+                    k_cheb_step<true, MW><<<grid_for(c, (const void*)k_cheb_step<true, MW>, n), NT,
+                                            0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st,
+                                                    c->d_part);
+                else
+                    k_cheb_step<false, MW><<<grid_for(c, (const void*)k_cheb_step<false, MW>, n),
+                                             NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j,
+                                                         c->d_st, c->d_part);
+                cudaEventRecord(ev[2 * k + 1], s);
+                ++k;
+                const cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) rc = fail(CF_ERR_CUDA, cudaGetErrorString(e));
+            }
+            if (rc != CF_OK) break;
+            k_pcg_p_spmv<MW><<<grid_for(c, (const void*)k_pcg_p_spmv<MW>, n), NT, 0, s>>>(
+                A, B, Z[chebz(7)], c->d_st, c->d_part);
+            k_pcg_update<true><<<grid_for(c, (const void*)k_pcg_update<true>, n), NT, 0, s>>>(
+                B, c->d_st, c->d_part, 0, 0);
+        }
+        double total = 0.0;
+        if (rc == CF_OK && cudaStreamSynchronize(s) == cudaSuccess)
+        {
+            for (int i = 0; i < k; ++i)
+            {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+                total += ms;
+            }
+            c->launches += (long long)reps * 9;
+        }
+        else if (rc == CF_OK)
+        {
+            rc = fail(CF_ERR_CUDA, "cudaStreamSynchronize");
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (rc != CF_OK) return rc;
+        *msPerLaunch = total / steps;
+        return CF_OK;
+    }
     auto launch = [&]() -> int {
         switch (which)
         {

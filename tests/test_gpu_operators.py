@@ -84,3 +84,25 @@ def test_bad_addressing_rejected(require_gpu):
         ctx.amul(np.zeros(a.n))
     assert ei.value.code == 3
     ctx.close()
+
+
+def test_time_kernel_modes(require_gpu):
+    """cf_time_kernel: every kernel id returns a positive time and leaves the
+    context usable; the in-iteration Chebyshev timing runs full PCG
+    iterations (9 launches each)."""
+    s = mesh.varcoeff3d((32, 30, 28), seed=11, permute=True)
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, None)
+    x = np.zeros(s.n)
+    ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, _lib.default_options(maxIter=3))
+    for k in ctx.KERNELS:
+        assert ctx.time_kernel(k, reps=4) > 0.0, k
+    l0 = ctx.kernel_launches()
+    ctx.time_kernel("cheb_step_inner", reps=3)
+    assert ctx.kernel_launches() - l0 >= 27
+    x = np.zeros(s.n)
+    p = ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, _lib.default_options())
+    assert p.converged
+    ctx.close()
