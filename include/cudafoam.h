@@ -340,10 +340,12 @@ enum
     CF_KERNEL_PCG_P_SPMV = 2,  /* p-update fused into the SpMV + p.Ap        */
     CF_KERNEL_PCG_UPDATE = 3,  /* delta/residual update + L1 + next apply    */
     CF_KERNEL_AMUL64 = 4,      /* FP64 refinement residual SpMV              */
-    CF_KERNEL_CHEB_STEP_INNER = 5 /* the Chebyshev steps inside `reps` full
+    CF_KERNEL_CHEB_STEP_INNER = 5, /* the Chebyshev steps inside `reps` full
                                      PCG iterations (order 8), each step
                                      bracketed by events: the cache state of
                                      a real solve, not of one kernel repeated */
+    CF_KERNEL_SPMV32_COLD = 6  /* FP32 SpMV + dot with L2 flushed (256 MB
+                                  read) before every timed launch           */
 };
 /* Launches one hot kernel `reps` times back to back on the context's stream
  * over the operands of the last solve (work vectors are overwritten, the

@@ -362,7 +362,7 @@ class Context:
         return y, d.value
 
     KERNELS = {"cheb_step": 0, "spmv32": 1, "pcg_p_spmv": 2, "pcg_update": 3, "amul64": 4,
-               "cheb_step_inner": 5}
+               "cheb_step_inner": 5, "spmv32_cold": 6}
 
     def time_kernel(self, which, reps=50):
         ms = C.c_double()

@@ -1111,6 +1111,20 @@ static __global__ void __launch_bounds__(NT) k_spmv32(DevSell A, const float* __
     if (grid_sum<1>(acc, part, ticket) && threadIdx.x == 0) *out = acc[0];
 }
 
+// Reads `count` float4 (an L2 flush that leaves only clean lines behind);
+// the sum is stored so the loads are not removed.
+static __global__ void k_read_flush(const float4* __restrict__ p, long long count, double* sink)
+{
+    float acc = 0.0f;
+    for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < count;
+         i += (long long)gridDim.x * NT)
+    {
+        const float4 v = __ldcg(p + i);
+        acc += v.x + v.y + v.z + v.w;
+    }
+    if (acc == 12345.0f) *sink = acc;
+}
+
 // cheb_init (metalFoamKernels.metal:154-171), writing w0 only (z0 = w0).
 static __global__ void k_cheb_init(int n, const float* __restrict__ r, const float* __restrict__ rD,
                             const float* __restrict__ chebC, float* __restrict__ w)
