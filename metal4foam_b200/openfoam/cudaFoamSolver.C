@@ -137,6 +137,7 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
         }
     }
 
+    (void)cmpt;   // every component of a segregated solve is a scalar system here
     solverPerformance solverPerf(solverName, fieldName_);
     cf_context* ctx = backend();
     FpTrapGuard fpe;
