@@ -343,7 +343,10 @@ enum
     CF_KERNEL_CHEB_STEP_INNER = 5, /* the Chebyshev steps inside `reps` full
                                      PCG iterations (order 8), each step
                                      bracketed by events: the cache state of
-                                     a real solve, not of one kernel repeated */
+                                     a real solve, not of one kernel repeated;
+                                     starts from the last solve's inner
+                                     right-hand side (CF_ERR_INVALID_ARG when
+                                     that is zero, e.g. before any solve)   */
     CF_KERNEL_SPMV32_COLD = 6  /* FP32 SpMV + dot with L2 flushed (256 MB
                                   read) before every timed launch           */
 };

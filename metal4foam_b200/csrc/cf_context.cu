@@ -671,6 +671,7 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
         c->clusterRemote = entries ? (double)remote / (double)entries : 0.0;
     }
     CF_CUDA(cudaMemsetAsync(c->d_D, 0, sizeof(float) * 3 * N, c->stream));
+    CF_CUDA(cudaMemsetAsync(c->d_r64, 0, sizeof(double) * N, c->stream));
     CF_CUDA(cudaStreamSynchronize(c->stream));
     c->hasTopo = true;
     c->lastLow = low;

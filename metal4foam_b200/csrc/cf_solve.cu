@@ -876,6 +876,14 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
         }
         for (auto& e : ev) cudaEventDestroy(e);
         if (rc != CF_OK) return rc;
+        // every timed step must have run its rows: a state that ended early
+        // (an inner right-hand side that is zero, as before any solve) would
+        // time kernels that return at once
+        CF_CUDA(cudaMemcpy(c->h_st, c->d_st, sizeof(InnerState), cudaMemcpyDeviceToHost));
+        if (c->h_st->done)
+            return fail(CF_ERR_INVALID_ARG,
+                        "cf_time_kernel(CHEB_STEP_INNER): the inner state ended before the timed "
+                        "iterations (zero inner right-hand side: run a solve first)");
         *msPerLaunch = total / steps;
         return CF_OK;
     }

@@ -95,6 +95,10 @@ def test_time_kernel_modes(require_gpu):
     a = s.addr
     ctx.set_topology(a.n, a.nf, *a.arrays())
     ctx.set_coeffs(s.diag, s.upper, None)
+    # before any solve there is no inner right-hand side to iterate on
+    with pytest.raises(_lib.CudaFoamError) as ei:
+        ctx.time_kernel("cheb_step_inner", reps=2)
+    assert ei.value.code == 1
     x = np.zeros(s.n)
     ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, _lib.default_options(maxIter=3))
     for k in ctx.KERNELS:
