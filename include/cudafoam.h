@@ -57,6 +57,12 @@ enum { CF_SOLVER_PCG = 0, CF_SOLVER_PBICGSTAB = 1 };
 /* deflate on|off|auto (metalFoamSolver.C:170-190) */
 enum { CF_DEFLATE_AUTO = 0, CF_DEFLATE_ON = 1, CF_DEFLATE_OFF = 2 };
 
+/* preconditioner of the inner FP32 PCG: the reference's Chebyshev-Jacobi
+ * polynomial of chebyshevOrder (default), or one aggregation multigrid
+ * V-cycle (no counterpart in the reference, whose README.md:221-227 lists
+ * GAMG as a limitation) */
+enum { CF_PRECOND_CHEBYSHEV = 0, CF_PRECOND_GAMG = 1 };
+
 /* internal cell ordering chosen at cf_set_topology */
 enum { CF_REORDER_NONE = 0, CF_REORDER_RCM = 1, CF_REORDER_AUTO = 2 };
 
@@ -111,6 +117,22 @@ typedef struct
                                   thread-block cluster of up to 16 CTAs,
                                   the work vectors in distributed shared
                                   memory; 0 (default) = 16384, < 0 = never */
+    int32_t preconditioner;    /* cudaPCG: CF_PRECOND_CHEBYSHEV (default) or
+                                  CF_PRECOND_GAMG: z = M r is one symmetric
+                                  V-cycle over aggregation levels (Galerkin
+                                  coarse operators summed on the device each
+                                  solve, Chebyshev-Jacobi smoothing on
+                                  [beta/chebyshevRatio, beta], the coarsest
+                                  level inverted densely); the FP64 driver
+                                  is unchanged.  Default SpMV shape only.  */
+    int32_t nSweeps;           /* GAMG: Chebyshev degree of the smoother,
+                                  2..8, default 3                          */
+    int32_t nCellsInCoarsestLevel; /* GAMG: coarsening stops at this many
+                                  cells or fewer, 1..128, default 128      */
+    double scaleCorrection;    /* GAMG: fixed factor on every coarse-grid
+                                  correction, in (0, 2) (the cycle stays
+                                  symmetric positive definite), default
+                                  1.8 (plain aggregation under-corrects)   */
 } cf_options;
 
 /* solverPerformance plus the reference's profile/verbose figures
@@ -144,7 +166,8 @@ int cf_abi_version(void);
 const char* cf_last_error(void);
 /* fills defaults: tolerance 1e-6, relTol 0, maxIter 1000, minIter 0,
  * maxRestarts 8, iterationsPerSync 1, deflate auto, chebyshevOrder 8,
- * chebyshevRatio 30, graph 1 */
+ * chebyshevRatio 30, graph 1, preconditioner Chebyshev, nSweeps 3,
+ * nCellsInCoarsestLevel 128, scaleCorrection 1.8 */
 void cf_options_default(cf_options* opts);
 
 /* ------------------------------------------------------------ context */
@@ -414,6 +437,13 @@ int cf_set_spmv_config(cf_context* ctx, const cf_spmv_config* cfg);
  * number of shapes timed. */
 int cf_autotune(cf_context* ctx, int32_t reps, int32_t apply, cf_spmv_config* best,
                 cf_tune_entry* table, int32_t capacity, int32_t* count);
+
+/* ------------------------------------------------------------ GAMG */
+/* Cells of every level of the context's multigrid hierarchy (built by the
+ * first cudaPCG solve with CF_PRECOND_GAMG on the current topology; level 0
+ * is the mesh): *levels receives the number of levels (0 before any GAMG
+ * solve), cells[0..min(levels, capacity)-1] their sizes. */
+int cf_gamg_levels(cf_context* ctx, int32_t* cells, int32_t capacity, int32_t* levels);
 
 /* ------------------------------------------------------------ no allocation */
 

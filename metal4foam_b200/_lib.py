@@ -22,6 +22,9 @@ STATUS = {
 CF_SOLVER_PCG = 0
 CF_SOLVER_PBICGSTAB = 1
 DEFLATE = {"auto": 0, "on": 1, "off": 2}
+CF_PRECOND_CHEBYSHEV = 0
+CF_PRECOND_GAMG = 1
+PRECONDITIONERS = {"Chebyshev": CF_PRECOND_CHEBYSHEV, "GAMG": CF_PRECOND_GAMG}
 REORDER = {"none": 0, "rcm": 1, "auto": 2}
 
 
@@ -48,6 +51,8 @@ class Options(C.Structure):
         ("stagnationLimit", C.c_int32),
         ("persistentMaxCells", C.c_int32),
         ("clusterMaxCells", C.c_int32),
+        ("preconditioner", C.c_int32), ("nSweeps", C.c_int32),
+        ("nCellsInCoarsestLevel", C.c_int32), ("scaleCorrection", C.c_double),
     ]
 
 
@@ -123,6 +128,7 @@ SIGNATURES = [
     ("cf_set_spmv_config", C.c_int, [vp, C.POINTER(SpmvConfig)]),
     ("cf_autotune", C.c_int, [vp, i32, i32, C.POINTER(SpmvConfig), C.POINTER(TuneEntry), i32,
                               C.POINTER(i32)]),
+    ("cf_gamg_levels", C.c_int, [vp, C.POINTER(i32), i32, C.POINTER(i32)]),
     ("cf_solve_multi", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
                                  C.POINTER(Performance)]),
     ("cf_solve_multi_device", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
@@ -204,6 +210,8 @@ def default_options(**kw):
     for k, v in kw.items():
         if k == "deflate" and isinstance(v, str):
             v = DEFLATE[v]
+        if k == "preconditioner" and isinstance(v, str):
+            v = PRECONDITIONERS[v]
         if isinstance(v, bool):
             v = int(v)
         if not hasattr(o, k):
@@ -379,6 +387,13 @@ class Context:
         keywords of :func:`spmv_config` (unnamed ones keep their defaults)."""
         k = cfg if cfg is not None else spmv_config(**kw)
         check(load().cf_set_spmv_config(self.h, C.byref(k)))
+
+    def gamg_levels(self):
+        """Cells per level of the GAMG hierarchy ([] before any GAMG solve)."""
+        cells = (C.c_int32 * 32)()
+        nl = C.c_int32()
+        check(load().cf_gamg_levels(self.h, cells, 32, C.byref(nl)))
+        return [cells[i] for i in range(min(nl.value, 32))]
 
     def autotune(self, reps=20, apply=True):
         """Times every SpMV launch shape on this matrix; returns (best

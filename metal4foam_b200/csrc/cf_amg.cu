@@ -1,0 +1,838 @@
+// cf_amg.cu -- aggregation multigrid V-cycle as the preconditioner of the
+// FP32 inner PCG (opt-in: cf_options.preconditioner = CF_PRECOND_GAMG).
+//
+// The reference has no such preconditioner (README.md:221-227 names GAMG
+// as a limitation of the Metal path); the driver around the inner solve
+// (FP64 residual, deflation, restarts, polish) is unchanged.  Only the
+// preconditioner apply z = M r of metalFoamBackend::pcg changes: the
+// Chebyshev-Jacobi polynomial (.C:342-385) is replaced by one symmetric
+// V-cycle, so PCG keeps a fixed SPD preconditioner.
+//
+// Hierarchy (built once per topology on the host): level 0 is the
+// context's matrix in its internal row order.  Each level's cells are
+// grouped into aggregates by root-based greedy aggregation on the cell
+// graph (a cell whose neighbours are all free becomes a root and takes
+// them; leftovers join a neighbouring aggregate); the aggregates, numbered
+// in the order their roots are met, are the next level's cells.  The
+// coarse operator is the Galerkin product P^T A P with the piecewise
+// constant P: a coarse face sums the fine faces between its two
+// aggregates, a coarse diagonal sums its cells' diagonals and twice the
+// faces inside it.  Coefficients are summed on the device for every solve
+// (segment sums in a fixed order, FP64), so a coefficient change needs no
+// host work.  The coarsest level (at most 128 cells) is inverted densely
+// (Gauss-Jordan, FP64) once per solve.
+//
+// V-cycle on level l (b = the level's right-hand side):
+//   x  = S(b)                  Chebyshev-Jacobi of degree nSweeps from 0
+//   r  = b - A x;  b' = P^T r;  x' = V-cycle(l+1, b');  x += P x'
+//   x += S(b - A x)            the same polynomial (symmetric cycle)
+// The smoother's interval is [beta/ratio, beta] with beta the Gershgorin
+// bound of D^-1 A on level 0 (metalFoamSolver.C:229-249) and ratio the
+// chebyshevRatio control; Galerkin levels of a diagonally dominant matrix
+// with non-positive off-diagonals keep that bound.  Level 0 reuses the
+// Krylov kernels (its pre-smoother start w0 = c1 rD r is formed by the
+// update kernel, its last post-smoothing step forms z.r and beta).
+#include "cudafoam.h"
+#include "cf_host.hpp"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cf_kernels.cuh"
+
+using namespace cf;
+
+#define AMG_CUDA(call)                                                          \
+    do                                                                          \
+    {                                                                           \
+        cudaError_t e_ = (call);                                                \
+        if (e_ != cudaSuccess)                                                  \
+            return fail(CF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define AMG_TRY(expr)                 \
+    do                                \
+    {                                 \
+        int rc_ = (expr);             \
+        if (rc_ != CF_OK) return rc_; \
+    } while (0)
+
+#define AMG_LAUNCH()                                                            \
+    do                                                                          \
+    {                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                    \
+        if (e_ != cudaSuccess)                                                  \
+            return fail(CF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+        c->launches++;                                                          \
+    } while (0)
+
+namespace cf {
+
+constexpr int AMG_MAX_COARSEST = 128;
+constexpr int AMG_MAX_LEVELS = 16;
+constexpr int AMG_INV_THREADS = 1024;
+constexpr int AMG_MAX_AGG = 8;       // cells per root aggregate at most
+
+struct AmgLevel
+{
+    int n = 0;
+    int nf = 0;                 // faces of this level (coarse levels: between aggregates)
+    // operator (levels >= 1; level 0 is the context's own)
+    DevSell A;
+    float* diag32 = nullptr;
+    float* rD32 = nullptr;
+    double* upper64 = nullptr;  // [nf] face coefficients (FP64)
+    double* diag64 = nullptr;   // [n]
+    int* eface = nullptr;       // SELL entry -> face
+    long long nnzp = 0;
+    // work vectors (levels >= 1)
+    float* b = nullptr;
+    float* x0 = nullptr;
+    float* x1 = nullptr;
+    float* w = nullptr;
+    float* r = nullptr;
+    // to the next level (absent on the coarsest)
+    int nagg = 0;
+    int* agg = nullptr;         // [n] aggregate of each row
+    int* aggStart = nullptr;    // [nagg + 1]
+    int* aggRows = nullptr;     // [n] rows by aggregate, ascending
+    int* cfStart = nullptr;     // [nf(l+1) + 1] this level's faces of each coarse face
+    int* cfList = nullptr;
+    int* intStart = nullptr;    // [nagg + 1] this level's faces inside each aggregate
+    int* intList = nullptr;
+};
+
+struct AmgData
+{
+    int coarsestCap = 0;        // nCellsInCoarsestLevel the hierarchy was built for
+    std::vector<AmgLevel> lv;
+    std::vector<void*> allocs;
+    double* coarseInv = nullptr;   // [nc * nc] inverse of the coarsest operator (row-major)
+    double* coarseWork = nullptr;  // [nc * nc] inversion workspace
+    float* scale = nullptr;        // scaleCorrection of the current solve
+    float hostScale = 1.0f;        // its host copy (source of the async upload)
+};
+
+namespace {
+
+template <class T>
+int amg_alloc(cf_context* c, AmgData* d, T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    const cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess)
+        return fail(CF_ERR_CUDA, std::string("cudaMalloc (multigrid): ") + cudaGetErrorString(e));
+    d->allocs.push_back((void*)*p);
+    (void)c;
+    return CF_OK;
+}
+
+template <class T>
+int amg_upload(cf_context* c, AmgData* d, T** p, const std::vector<T>& h)
+{
+    AMG_TRY(amg_alloc(c, d, p, h.size()));
+    if (!h.empty())
+        AMG_CUDA(cudaMemcpyAsync(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice,
+                                 c->stream));
+    return CF_OK;
+}
+
+// Root-based greedy aggregation of an undirected graph (CSR adjacency).
+// A root takes at most AMG_MAX_AGG - 1 neighbours, so coarse levels, whose
+// graphs are denser, still coarsen by a factor of about 8 per level.
+int aggregate(int n, const std::vector<int>& xadj, const std::vector<int>& adj,
+              std::vector<int>& agg)
+{
+    agg.assign(n, -1);
+    int nagg = 0;
+    // roots: a free cell whose neighbours are all free takes (up to the cap of) them
+    for (int i = 0; i < n; ++i)
+    {
+        if (agg[i] >= 0) continue;
+        bool free = true;
+        for (int q = xadj[i]; q < xadj[i + 1] && free; ++q) free = agg[adj[q]] < 0;
+        if (!free) continue;
+        agg[i] = nagg;
+        int taken = 1;
+        for (int q = xadj[i]; q < xadj[i + 1] && taken < AMG_MAX_AGG; ++q, ++taken)
+            agg[adj[q]] = nagg;
+        ++nagg;
+    }
+    // leftovers join the first aggregated neighbour (decided against the
+    // root phase's assignment only, so the order of the sweep does not chain)
+    std::vector<int> join(n, -1);
+    for (int i = 0; i < n; ++i)
+    {
+        if (agg[i] >= 0) continue;
+        for (int q = xadj[i]; q < xadj[i + 1]; ++q)
+            if (agg[adj[q]] >= 0)
+            {
+                join[i] = agg[adj[q]];
+                break;
+            }
+    }
+    for (int i = 0; i < n; ++i)
+        if (agg[i] < 0 && join[i] >= 0) agg[i] = join[i];
+    // cells with no aggregated neighbour: new aggregates with their free neighbours
+    for (int i = 0; i < n; ++i)
+    {
+        if (agg[i] >= 0) continue;
+        agg[i] = nagg;
+        for (int q = xadj[i]; q < xadj[i + 1]; ++q)
+            if (agg[adj[q]] < 0) agg[adj[q]] = nagg;
+        ++nagg;
+    }
+    return nagg;
+}
+
+void csr_of_faces(int n, const std::vector<int>& lo, const std::vector<int>& up,
+                  std::vector<int>& xadj, std::vector<int>& adj)
+{
+    xadj.assign(n + 1, 0);
+    for (size_t f = 0; f < lo.size(); ++f)
+    {
+        ++xadj[lo[f] + 1];
+        ++xadj[up[f] + 1];
+    }
+    for (int i = 0; i < n; ++i) xadj[i + 1] += xadj[i];
+    adj.assign(xadj[n], 0);
+    std::vector<int> pos(xadj.begin(), xadj.end() - 1);
+    for (size_t f = 0; f < lo.size(); ++f)
+    {
+        adj[pos[lo[f]]++] = up[f];
+        adj[pos[up[f]]++] = lo[f];
+    }
+}
+
+// ---------------------------------------------------------------- kernels
+
+// coarse face coefficient: the sum of the fine faces between its aggregates
+__global__ void ka_coarse_upper(int nfc, const int* __restrict__ start, const int* __restrict__ list,
+                                const double* __restrict__ upper, double* __restrict__ out)
+{
+    for (int F = blockIdx.x * NT + threadIdx.x; F < nfc; F += gridDim.x * NT)
+    {
+        double s = 0.0;
+        for (int q = start[F]; q < start[F + 1]; ++q) s += upper[list[q]];
+        out[F] = s;
+    }
+}
+
+// coarse diagonal: the cells' diagonals plus both sides of the inner faces.
+// Level 0's diagonal is diag64 - u when the driver deflates (the staged
+// FP32 operator of metalFoamSolver.C:197-209).
+__global__ void ka_coarse_diag(int nagg, const int* __restrict__ aggStart,
+                               const int* __restrict__ aggRows, const int* __restrict__ intStart,
+                               const int* __restrict__ intList, const double* __restrict__ diag,
+                               const double* __restrict__ u, int deflate,
+                               const double* __restrict__ upper, double* __restrict__ out64,
+                               float* __restrict__ out32, float* __restrict__ rD32)
+{
+    for (int K = blockIdx.x * NT + threadIdx.x; K < nagg; K += gridDim.x * NT)
+    {
+        double s = 0.0;
+        for (int q = aggStart[K]; q < aggStart[K + 1]; ++q)
+        {
+            const int i = aggRows[q];
+            s += deflate ? __dsub_rn(diag[i], u[i]) : diag[i];
+        }
+        for (int q = intStart[K]; q < intStart[K + 1]; ++q) s += 2.0 * upper[intList[q]];
+        out64[K] = s;
+        out32[K] = (float)s;
+        rD32[K] = (float)(1.0 / s);
+    }
+}
+
+// symmetric SELL values of a coarse level
+__global__ void ka_stage_vals(long long nnzp, const int* __restrict__ eface,
+                              const double* __restrict__ upper, float* __restrict__ val)
+{
+    for (long long e = (long long)blockIdx.x * NT + threadIdx.x; e < nnzp;
+         e += (long long)gridDim.x * NT)
+    {
+        const int f = eface[e];
+        val[e] = f < 0 ? 0.0f : (float)upper[f];
+    }
+}
+
+// dense coarsest operator (+ s 11^T when it is singular by construction),
+// then its inverse by Gauss-Jordan without pivoting (SPD), one block
+__global__ void __launch_bounds__(AMG_INV_THREADS)
+    ka_coarse_invert(int nc, const int* __restrict__ sliceOff, const int* __restrict__ col,
+                     const int* __restrict__ eface, const double* __restrict__ upper,
+                     const double* __restrict__ diag, int shift, double* __restrict__ M,
+                     double* __restrict__ inv)
+{
+    const int t = threadIdx.x;
+    for (int k = t; k < nc * nc; k += blockDim.x)
+    {
+        M[k] = 0.0;
+        inv[k] = ((k / nc) == (k % nc)) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    double dsum = 0.0;
+    for (int i = 0; i < nc; ++i) dsum += diag[i];
+    const double s = shift ? dsum / ((double)nc * (double)nc) : 0.0;
+    for (int i = t; i < nc; i += blockDim.x)
+    {
+        M[i * nc + i] += diag[i];
+        const int sl = i / SLICE;
+        const int w = (sliceOff[sl + 1] - sliceOff[sl]) / SLICE;
+        for (int k = 0; k < w; ++k)
+        {
+            const int e = sliceOff[sl] + SLICE * k + (i % SLICE);
+            const int cc = col[e];
+            if (cc == -1) continue;
+            M[i * nc + col_index(cc)] += upper[eface[e]];
+        }
+    }
+    __syncthreads();
+    if (shift)
+    {
+        for (int k = t; k < nc * nc; k += blockDim.x) M[k] += s;
+        __syncthreads();
+    }
+    for (int p = 0; p < nc; ++p)
+    {
+        const double piv = M[p * nc + p];
+        __syncthreads();
+        for (int j = t; j < nc; j += blockDim.x)
+        {
+            M[p * nc + j] /= piv;
+            inv[p * nc + j] /= piv;
+        }
+        __syncthreads();
+        for (int k = t; k < nc * nc; k += blockDim.x)
+        {
+            const int i = k / nc;
+            const int j = k % nc;
+            if (i == p) continue;
+            const double f = M[i * nc + p];
+            if (j != p) M[k] -= f * M[p * nc + j];
+            inv[k] -= f * inv[p * nc + j];
+        }
+        __syncthreads();
+        for (int i = t; i < nc; i += blockDim.x)
+            if (i != p) M[i * nc + p] = 0.0;
+        __syncthreads();
+    }
+}
+
+// x = inv b on the coarsest level (one block)
+__global__ void __launch_bounds__(NT) ka_coarse_solve(int nc, const double* __restrict__ inv,
+                                                      const float* __restrict__ b,
+                                                      float* __restrict__ x,
+                                                      const InnerState* st)
+{
+    if (st->done) return;
+    for (int i = threadIdx.x; i < nc; i += NT)
+    {
+        double s = 0.0;
+        for (int j = 0; j < nc; ++j) s += inv[i * nc + j] * (double)b[j];
+        x[i] = (float)s;
+    }
+}
+
+// One FP32 row of a coarse level's operator (32-bit column stream; the
+// Galerkin rows hold up to ~26 entries): chunks of 8 entries whose loads
+// are independent, products added in entry order.
+template <class XF>
+__device__ __forceinline__ float row_coarse(const DevSell& A, int row, float acc, XF xf)
+{
+    const int sl = row >> 5;
+    const int b0 = A.ellW ? sl * SLICE * A.ellW : __ldg(A.sliceOff + sl);
+    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + sl + 1) - b0) >> 5;
+    const int base = b0 + (row & 31);
+    for (int k0 = 0; k0 < w; k0 += 8)
+    {
+        int c[8];
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            if (k0 + k < w)
+            {
+                c[k] = __ldcs(A.col + base + SLICE * (k0 + k));
+                v[k] = __ldcs(A.val + base + SLICE * (k0 + k));
+            }
+            else
+            {
+                c[k] = -1;
+                v[k] = 0.0f;
+            }
+        }
+        float x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = (c[k] != -1) ? xf(col_index(c[k])) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (c[k] != -1) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
+    }
+    return acc;
+}
+
+// the row of level 0 (the context's layout) or of a coarse level
+template <int MAXW, bool COARSE, class XF>
+__device__ __forceinline__ float row_level(const DevSell& A, int row, float acc, XF xf)
+{
+    if (COARSE) return row_coarse(A, row, acc, xf);
+    return row_f32<MAXW>(A, row, acc, xf);
+}
+
+// x = w = c1 rD b
+__global__ void __launch_bounds__(NT) ka_init(int n, const float* __restrict__ rD,
+                                              const float* __restrict__ b,
+                                              const float* __restrict__ cc, float* __restrict__ x,
+                                              float* __restrict__ w, const InnerState* st)
+{
+    if (st->done) return;
+    const float c1 = cc[0];
+    CF_ROWS(row, n)
+    {
+        const float v = __fmul_rn(__fmul_rn(c1, rD[row]), b[row]);
+        x[row] = v;
+        w[row] = v;
+    }
+}
+
+// Chebyshev step j >= 1:  w = c2 w + c3 rD (b - A xin);  xout = xin + w.
+// j = 0 starts the post-smoother from xin:  w = c1 rD (b - A xin).
+template <int MAXW, bool COARSE>
+__global__ void __launch_bounds__(NT) ka_step(DevSell A, const float* __restrict__ diag,
+                                              const float* __restrict__ rD,
+                                              const float* __restrict__ b, const float* xin,
+                                              float* w, float* xout,
+                                              const float* __restrict__ cc, int j,
+                                              const InnerState* st)
+{
+    if (st->done) return;
+    const float c2 = j > 0 ? cc[2 * j - 1] : 0.0f;
+    const float c3 = j > 0 ? cc[2 * j] : cc[0];
+    CF_ROWS(row, A.n)
+    {
+        const float xr = xin[row];
+        const float v = row_level<MAXW, COARSE>(A, row, __fmul_rn(diag[row], xr),
+                                                [&](int q) { return __ldg(xin + q); });
+        const float s = __fmul_rn(__fmul_rn(c3, rD[row]), __fsub_rn(b[row], v));
+        const float wn = j > 0 ? __fadd_rn(__fmul_rn(c2, w[row]), s) : s;
+        w[row] = wn;
+        xout[row] = __fadd_rn(xr, wn);
+    }
+}
+
+// r = b - A x
+template <int MAXW, bool COARSE>
+__global__ void __launch_bounds__(NT) ka_resid(DevSell A, const float* __restrict__ diag,
+                                               const float* __restrict__ b,
+                                               const float* __restrict__ x, float* __restrict__ r,
+                                               const InnerState* st)
+{
+    if (st->done) return;
+    CF_ROWS(row, A.n)
+    {
+        const float v = row_level<MAXW, COARSE>(A, row, __fmul_rn(diag[row], x[row]),
+                                                [&](int q) { return __ldg(x + q); });
+        r[row] = __fsub_rn(b[row], v);
+    }
+}
+
+// b' = P^T r: per aggregate, the sum of its rows in ascending order
+__global__ void __launch_bounds__(NT) ka_restrict(int nagg, const int* __restrict__ aggStart,
+                                                  const int* __restrict__ aggRows,
+                                                  const float* __restrict__ r,
+                                                  float* __restrict__ bc, const InnerState* st)
+{
+    if (st->done) return;
+    for (int K = blockIdx.x * NT + threadIdx.x; K < nagg; K += gridDim.x * NT)
+    {
+        float s = 0.0f;
+        for (int q = aggStart[K]; q < aggStart[K + 1]; ++q) s = __fadd_rn(s, r[aggRows[q]]);
+        bc[K] = s;
+    }
+}
+
+// x += a P x' (a = scaleCorrection; a fixed factor keeps the cycle a
+// fixed symmetric operator, positive definite for 0 < a < 2)
+__global__ void __launch_bounds__(NT) ka_prolong(int n, const int* __restrict__ agg,
+                                                 const float* __restrict__ xc,
+                                                 const float* __restrict__ scale,
+                                                 float* __restrict__ x, const InnerState* st)
+{
+    if (st->done) return;
+    const float a = *scale;
+    CF_ROWS(row, n) x[row] = __fadd_rn(x[row], __fmul_rn(a, xc[agg[row]]));
+}
+
+constexpr int MW = MAXW_UNROLL;
+
+int grid_n(cf_context* c, const void* fn, long long n) { return grid_for(c, fn, n); }
+
+// Level l >= 1 of the V-cycle on its own buffers; returns the buffer
+// holding the level's correction.
+int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
+{
+    AmgLevel& L = d->lv[l];
+    cudaStream_t s = c->stream;
+    const InnerState* st = c->d_st;
+    const int last = (int)d->lv.size() - 1;
+    if (l == last)
+    {
+        ka_coarse_solve<<<1, NT, 0, s>>>(L.n, d->coarseInv, L.b, L.x0, st);
+        AMG_LAUNCH();
+        *result = L.x0;
+        return CF_OK;
+    }
+    const float* cc = c->d_chebC;
+    // pre-smoothing from zero
+    ka_init<<<grid_n(c, (const void*)ka_init, L.n), NT, 0, s>>>(L.n, L.rD32, L.b, cc, L.x0, L.w, st);
+    AMG_LAUNCH();
+    float* xa = L.x0;
+    float* xb = L.x1;
+    for (int j = 1; j < degree; ++j)
+    {
+        ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
+            L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
+        AMG_LAUNCH();
+        std::swap(xa, xb);
+    }
+    // coarse-grid correction
+    ka_resid<MW, true><<<grid_n(c, (const void*)ka_resid<MW, true>, L.n), NT, 0, s>>>(
+        L.A, L.diag32, L.b, xa, L.r, st);
+    AMG_LAUNCH();
+    AmgLevel& N = d->lv[l + 1];
+    ka_restrict<<<grid_n(c, (const void*)ka_restrict, L.nagg), NT, 0, s>>>(L.nagg, L.aggStart,
+                                                                           L.aggRows, L.r, N.b, st);
+    AMG_LAUNCH();
+    float* xc = nullptr;
+    AMG_TRY(vcycle_coarse(c, d, l + 1, degree, &xc));
+    ka_prolong<<<grid_n(c, (const void*)ka_prolong, L.n), NT, 0, s>>>(L.n, L.agg, xc, d->scale,
+                                                                      xa, st);
+    AMG_LAUNCH();
+    // post-smoothing from x
+    for (int j = 0; j < degree; ++j)
+    {
+        ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
+            L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
+        AMG_LAUNCH();
+        std::swap(xa, xb);
+    }
+    *result = xa;
+    return CF_OK;
+}
+
+}  // namespace
+
+void amg_release(cf_context* c)
+{
+    AmgData* d = static_cast<AmgData*>(c->amg);
+    if (!d) return;
+    for (void* p : d->allocs) cudaFree(p);
+    delete d;
+    c->amg = nullptr;
+}
+
+int amg_levels(const cf_context* c)
+{
+    const AmgData* d = static_cast<const AmgData*>(c->amg);
+    return d ? (int)d->lv.size() : 0;
+}
+
+int amg_level_cells(const cf_context* c, int l)
+{
+    const AmgData* d = static_cast<const AmgData*>(c->amg);
+    return (d && l >= 0 && l < (int)d->lv.size()) ? d->lv[l].n : 0;
+}
+
+// Hierarchy of the context's topology (host aggregation, device layouts).
+int amg_prepare(cf_context* c, int coarsestCap)
+{
+    AmgData* old = static_cast<AmgData*>(c->amg);
+    if (old && old->coarsestCap == coarsestCap) return CF_OK;
+    amg_release(c);
+    AmgData* d = new AmgData();
+    c->amg = d;
+    d->coarsestCap = coarsestCap;
+    const int n = c->n;
+    const int nf = c->nf;
+    // level-0 faces in the internal row order (the caller's face order kept,
+    // so face f addresses the caller's upper[f])
+    std::vector<int> lo(nf), up(nf);
+    if (nf > 0)
+    {
+        AMG_CUDA(cudaMemcpyAsync(lo.data(), c->d_low, sizeof(int) * nf, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        AMG_CUDA(cudaMemcpyAsync(up.data(), c->d_upp, sizeof(int) * nf, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        AMG_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    {
+        std::vector<int> iperm(n);
+        for (int r = 0; r < n; ++r) iperm[c->perm[r]] = r;
+        for (int f = 0; f < nf; ++f)
+        {
+            lo[f] = iperm[lo[f]];
+            up[f] = iperm[up[f]];
+        }
+    }
+    d->lv.emplace_back();
+    d->lv[0].n = n;
+    d->lv[0].nf = nf;
+    int cur = 0;
+    while ((int)d->lv.size() < AMG_MAX_LEVELS && d->lv[cur].n > coarsestCap)
+    {
+        const int nl = d->lv[cur].n;
+        const int nfl = (int)lo.size();
+        std::vector<int> xadj, adj, agg;
+        csr_of_faces(nl, lo, up, xadj, adj);
+        const int nagg = aggregate(nl, xadj, adj, agg);
+        if (nagg >= nl || nagg < 1) break;   // no coarsening possible
+        // members of each aggregate (ascending rows)
+        std::vector<int> aggStart(nagg + 1, 0), aggRows(nl);
+        for (int i = 0; i < nl; ++i) ++aggStart[agg[i] + 1];
+        for (int k = 0; k < nagg; ++k) aggStart[k + 1] += aggStart[k];
+        {
+            std::vector<int> pos(aggStart.begin(), aggStart.end() - 1);
+            for (int i = 0; i < nl; ++i) aggRows[pos[agg[i]]++] = i;
+        }
+        // faces inside aggregates, and coarse faces (owner < neighbour, sorted)
+        std::vector<int> intStart(nagg + 1, 0), intList;
+        std::vector<std::pair<uint64_t, int>> between;
+        between.reserve(nfl);
+        for (int f = 0; f < nfl; ++f)
+        {
+            const int a = agg[lo[f]];
+            const int b = agg[up[f]];
+            if (a == b)
+                ++intStart[a + 1];
+            else
+                between.push_back({((uint64_t)std::min(a, b) << 32) | (uint64_t)std::max(a, b), f});
+        }
+        for (int k = 0; k < nagg; ++k) intStart[k + 1] += intStart[k];
+        intList.assign(intStart[nagg], 0);
+        {
+            std::vector<int> pos(intStart.begin(), intStart.end() - 1);
+            for (int f = 0; f < nfl; ++f)
+            {
+                const int a = agg[lo[f]];
+                if (a == agg[up[f]]) intList[pos[a]++] = f;
+            }
+        }
+        std::sort(between.begin(), between.end());
+        std::vector<int> clo, cup, cfStart, cfList(between.size());
+        for (size_t q = 0; q < between.size(); ++q)
+        {
+            if (q == 0 || between[q].first != between[q - 1].first)
+            {
+                cfStart.push_back((int)q);
+                clo.push_back((int)(between[q].first >> 32));
+                cup.push_back((int)(between[q].first & 0xffffffffu));
+            }
+            cfList[q] = between[q].second;
+        }
+        cfStart.push_back((int)between.size());
+        const int nfc = (int)clo.size();
+
+        AmgLevel& L = d->lv[cur];
+        L.nagg = nagg;
+        AMG_TRY(amg_upload(c, d, &L.agg, agg));
+        AMG_TRY(amg_upload(c, d, &L.aggStart, aggStart));
+        AMG_TRY(amg_upload(c, d, &L.aggRows, aggRows));
+        AMG_TRY(amg_upload(c, d, &L.intStart, intStart));
+        AMG_TRY(amg_upload(c, d, &L.intList, intList));
+        AMG_TRY(amg_upload(c, d, &L.cfStart, cfStart));
+        AMG_TRY(amg_upload(c, d, &L.cfList, cfList));
+
+        // the coarse level's LDU addressing and SELL layout (identity order)
+        std::vector<int> own(nagg + 1, 0), losS(nagg + 1, 0), los(nfc);
+        for (int F = 0; F < nfc; ++F)
+        {
+            ++own[clo[F] + 1];
+            ++losS[cup[F] + 1];
+        }
+        for (int k = 0; k < nagg; ++k)
+        {
+            own[k + 1] += own[k];
+            losS[k + 1] += losS[k];
+        }
+        {
+            std::vector<int> pos(losS.begin(), losS.end() - 1);
+            for (int F = 0; F < nfc; ++F) los[pos[cup[F]]++] = F;
+        }
+        HostLayout H;
+        AMG_TRY(build_layout(nagg, nfc, clo.data(), cup.data(), own.data(), los.data(),
+                             losS.data(), false, H));
+        d->lv.emplace_back();
+        AmgLevel& C = d->lv.back();
+        C.n = nagg;
+        C.nf = nfc;
+        C.nnzp = H.nnzp;
+        int* sliceOff = nullptr;
+        int* col = nullptr;
+        float* val = nullptr;
+        AMG_TRY(amg_upload(c, d, &sliceOff, H.sliceOff));
+        AMG_TRY(amg_upload(c, d, &col, H.col));
+        AMG_TRY(amg_upload(c, d, &C.eface, H.eface));
+        AMG_TRY(amg_alloc(c, d, &val, (size_t)std::max(H.nnzp, 1LL)));
+        C.A.n = nagg;
+        C.A.nslices = H.nslices;
+        C.A.sliceOff = sliceOff;
+        C.A.col = col;
+        C.A.val = val;
+        C.A.val64 = nullptr;
+        C.A.col16 = nullptr;
+        C.A.ellW = H.uniformW;
+        AMG_TRY(amg_alloc(c, d, &C.diag32, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.rD32, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.diag64, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.upper64, nfc));
+        AMG_TRY(amg_alloc(c, d, &C.b, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.x0, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.x1, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.w, nagg));
+        AMG_TRY(amg_alloc(c, d, &C.r, nagg));
+        lo.swap(clo);
+        up.swap(cup);
+        cur = (int)d->lv.size() - 1;
+        if (nagg * 10 > nl * 9) break;   // coarsening stalled
+    }
+    AmgLevel& Z = d->lv.back();
+    if (d->lv.size() < 2 || Z.n > AMG_MAX_COARSEST)
+    {
+        amg_release(c);
+        return fail(CF_ERR_UNSUPPORTED,
+                    "GAMG: the mesh does not coarsen to at most 128 cells (disconnected or "
+                    "too few faces)");
+    }
+    AMG_TRY(amg_alloc(c, d, &d->scale, 1));
+    AMG_TRY(amg_alloc(c, d, &d->coarseInv, (size_t)Z.n * Z.n));
+    AMG_TRY(amg_alloc(c, d, &d->coarseWork, (size_t)Z.n * Z.n));
+    AMG_CUDA(cudaStreamSynchronize(c->stream));
+    return CF_OK;
+}
+
+// Coefficients of every coarse level from the staged operator of level 0
+// (diag64, or diag64 - u when deflating; the caller's upper).
+int amg_stage(cf_context* c, int deflate, float scaleCorrection)
+{
+    AmgData* d = static_cast<AmgData*>(c->amg);
+    if (!d) return fail(CF_ERR_INVALID_ARG, "GAMG hierarchy not built");
+    cudaStream_t s = c->stream;
+    d->hostScale = scaleCorrection;
+    AMG_CUDA(cudaMemcpyAsync(d->scale, &d->hostScale, sizeof(float), cudaMemcpyHostToDevice, s));
+    for (size_t l = 0; l + 1 < d->lv.size(); ++l)
+    {
+        AmgLevel& F = d->lv[l];
+        AmgLevel& C = d->lv[l + 1];
+        const double* upper = l == 0 ? c->d_upper : F.upper64;
+        const double* diag = l == 0 ? c->d_diag64 : F.diag64;
+        ka_coarse_upper<<<grid_n(c, (const void*)ka_coarse_upper, C.nf), NT, 0, s>>>(
+            C.nf, F.cfStart, F.cfList, upper, C.upper64);
+        AMG_LAUNCH();
+        ka_coarse_diag<<<grid_n(c, (const void*)ka_coarse_diag, C.n), NT, 0, s>>>(
+            C.n, F.aggStart, F.aggRows, F.intStart, F.intList, diag, c->d_u,
+            (l == 0 && deflate) ? 1 : 0, upper, C.diag64, C.diag32, C.rD32);
+        AMG_LAUNCH();
+        ka_stage_vals<<<grid_n(c, (const void*)ka_stage_vals, C.nnzp), NT, 0, s>>>(
+            C.nnzp, C.eface, C.upper64, const_cast<float*>(C.A.val));
+        AMG_LAUNCH();
+    }
+    AmgLevel& Z = d->lv.back();
+    ka_coarse_invert<<<1, AMG_INV_THREADS, 0, s>>>(Z.n, Z.A.sliceOff, Z.A.col, Z.eface, Z.upper64,
+                                                   Z.diag64, deflate ? 1 : 0, d->coarseWork,
+                                                   d->coarseInv);
+    AMG_LAUNCH();
+    return CF_OK;
+}
+
+// One inner PCG iteration with the V-cycle: z = M r, then the p-update SpMV
+// and the update of metalFoamBackend::pcg (.C:676-715).
+int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int useCond,
+                    int* kernels)
+{
+    AmgData* d = static_cast<AmgData*>(c->amg);
+    if (!d || d->lv.size() < 2) return fail(CF_ERR_INVALID_ARG, "GAMG hierarchy not built");
+    const long long l0 = c->launches;
+    const DevSell A = sell_of(c);
+    const PcgBufs B = pcg_bufs(c);
+    cudaStream_t s = c->stream;
+    float* Z[2] = {B.Z0, B.Z1};
+    // level 0 pre-smoothing: w0 = c1 rD r is in W0 (formed by the update)
+    const float* xa = B.W0;
+    int zi = 0;
+    for (int j = 1; j < degree; ++j)
+    {
+        auto fn = k_cheb_step<false, MW>;
+        fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, xa, j == 1 ? B.W0 : B.W1, B.W1,
+                                                            Z[zi], j, c->d_st, c->d_part);
+        AMG_LAUNCH();
+        xa = Z[zi];
+        zi ^= 1;
+    }
+    float* x0 = const_cast<float*>(xa);
+    // coarse-grid correction (the residual in Q, free until the p-update SpMV)
+    ka_resid<MW, false><<<grid_for(c, (const void*)ka_resid<MW, false>, c->n), NT, 0, s>>>(
+        A, B.diag, B.rA, x0, B.Q, c->d_st);
+    AMG_LAUNCH();
+    AmgLevel& L0 = d->lv[0];
+    ka_restrict<<<grid_for(c, (const void*)ka_restrict, L0.nagg), NT, 0, s>>>(
+        L0.nagg, L0.aggStart, L0.aggRows, B.Q, d->lv[1].b, c->d_st);
+    AMG_LAUNCH();
+    float* xc = nullptr;
+    AMG_TRY(vcycle_coarse(c, d, 1, degree, &xc));
+    ka_prolong<<<grid_for(c, (const void*)ka_prolong, c->n), NT, 0, s>>>(c->n, L0.agg, xc,
+                                                                         d->scale, x0, c->d_st);
+    AMG_LAUNCH();
+    // level 0 post-smoothing; the last step forms z.r and beta
+    float* xin = x0;
+    float* xout = (x0 == Z[0]) ? Z[1] : Z[0];
+    ka_step<MW, false><<<grid_for(c, (const void*)ka_step<MW, false>, c->n), NT, 0, s>>>(
+        A, B.diag, B.rD, B.rA, xin, B.W1, xout, c->d_chebC, 0, c->d_st);
+    AMG_LAUNCH();
+    std::swap(xin, xout);
+    for (int j = 1; j < degree; ++j)
+    {
+        if (j == degree - 1)
+        {
+            auto fn = k_cheb_step<true, MW>;
+            fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, xin, B.W1, B.W1, xout, j,
+                                                                c->d_st, c->d_part);
+        }
+        else
+        {
+            auto fn = k_cheb_step<false, MW>;
+            fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, xin, B.W1, B.W1, xout, j,
+                                                                c->d_st, c->d_part);
+        }
+        AMG_LAUNCH();
+        std::swap(xin, xout);
+    }
+    const float* z = xin;
+    {
+        auto fn = k_pcg_p_spmv<MW>;
+        fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, z, c->d_st, c->d_part);
+        AMG_LAUNCH();
+    }
+    {
+        auto fn = k_pcg_update<true>;
+        fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(B, c->d_st, c->d_part, h, useCond);
+        AMG_LAUNCH();
+    }
+    if (kernels) *kernels = (int)(c->launches - l0);
+    return CF_OK;
+}
+
+}  // namespace cf
+
+extern "C" int cf_gamg_levels(cf_context* c, int32_t* cells, int32_t capacity, int32_t* levels)
+{
+    if (!c || !levels || (capacity > 0 && !cells))
+        return fail(CF_ERR_INVALID_ARG, "NULL argument");
+    const int L = amg_levels(c);
+    *levels = L;
+    for (int l = 0; l < L && l < capacity; ++l) cells[l] = amg_level_cells(c, l);
+    return CF_OK;
+}

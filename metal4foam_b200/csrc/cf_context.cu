@@ -84,6 +84,7 @@ int dalloc(cf_context* c, T** p, size_t count)
 void free_topology(cf_context* c)
 {
     cf_multi_release(c);
+    amg_release(c);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();
     for (void* p : c->topoAllocs) cudaFree(p);
@@ -406,6 +407,10 @@ extern "C" void cf_options_default(cf_options* o)
     o->profile = 0;
     o->verbose = 0;
     o->graph = 1;
+    o->preconditioner = CF_PRECOND_CHEBYSHEV;
+    o->nSweeps = 3;
+    o->nCellsInCoarsestLevel = 128;
+    o->scaleCorrection = 1.8;
 }
 
 extern "C" int cf_context_create(cf_context** out, int32_t device)

@@ -102,6 +102,7 @@ struct cf_context
 
     // instantiated inner-loop graphs keyed by (kind, chebyshev order)
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    std::map<std::pair<int, int>, int> graphKernels;   // kernels in each graph's loop body
 
     // several right-hand sides on this matrix (cf_multi.cu), built on first use
     void* multi = nullptr;
@@ -110,6 +111,8 @@ struct cf_context
     // (CF_LAYOUT_*), rows per warp, block size, multi-RHS tile
     int maxCtasPerSM = 32;
     bool coopLaunch = false;               // device supports cooperative launches
+    void* amg = nullptr;                   // GAMG hierarchy of the topology (cf_amg.cu)
+    bool amgActive = false;                // inner PCG iterations use the V-cycle
     int clusterShift = 10;                 // log2(rows per CTA) of the cluster PCG for this mesh
     double clusterRemote = 1.0;            // fraction of entries whose column lies in another CTA
     unsigned int* d_bar = nullptr;         // grid barrier of persistent inner solves: count, generation, error
@@ -192,5 +195,17 @@ int cluster_inner(cf_context* c, int order, int maxCells, bool* ran);
 // power of two >= 32 that needs at most 16 CTAs.
 int cluster_shift(int n);
 int persistent_status(cf_context* c);
+
+// Aggregation multigrid preconditioner of the inner PCG (cf_amg.cu):
+// hierarchy of the topology down to at most coarsestCap (<= 128) cells,
+// coefficients of every level from the staged operator (deflated or not),
+// and one inner iteration with the V-cycle as z = M r.
+int amg_prepare(cf_context* c, int coarsestCap);
+int amg_stage(cf_context* c, int deflate, float scaleCorrection);
+int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int useCond,
+                    int* kernels);
+int amg_levels(const cf_context* c);
+int amg_level_cells(const cf_context* c, int level);
+void amg_release(cf_context* c);
 
 }  // namespace cf

@@ -47,6 +47,7 @@ int chebz(int j) { return j & 1; }
 int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int useCond,
                     int* kernels)
 {
+    if (c->amgActive) return launch_amg_body(c, order, h, useCond, kernels);
     const DevSell A = sell_of(c);
     const PcgBufs B = pcg_bufs(c);
     cudaStream_t s = c->stream;
@@ -143,12 +144,13 @@ int launch_bicg_body(cf_context* c, cudaGraphConditionalHandle h, int useCond, i
 // the body sets the condition from the device-side convergence state.
 int get_graph(cf_context* c, int kind, int order, cudaGraphExec_t* out, int* bodyKernels)
 {
-    const auto key = std::make_pair(kind, kind == 0 ? order : 1);
+    // (kind 2: PCG whose preconditioner is the multigrid V-cycle)
+    const auto key = std::make_pair(kind == 0 && c->amgActive ? 2 : kind, kind == 0 ? order : 1);
     auto it = c->graphs.find(key);
     if (it != c->graphs.end())
     {
         *out = it->second;
-        *bodyKernels = kind == 0 ? (order > 1 ? order + 1 : 2) : 3;
+        *bodyKernels = c->graphKernels[key];
         return CF_OK;
     }
     cudaGraph_t g = nullptr;
@@ -204,6 +206,7 @@ int get_graph(cf_context* c, int kind, int order, cudaGraphExec_t* out, int* bod
     if (e != cudaSuccess)
         return fail(CF_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
     c->graphs[key] = exec;
+    c->graphKernels[key] = nk;
     *out = exec;
     *bodyKernels = nk;
     return CF_OK;
@@ -250,10 +253,10 @@ int inner_solve(cf_context* c, int kind, const double* mean, double target, int 
     if (maxIter > 0)
     {
         // small PCG systems: the whole loop inside one thread-block cluster
-        if (useGraph && spmv_default(c) && kind == 0 && clusterMax >= 0)
+        if (useGraph && spmv_default(c) && kind == 0 && clusterMax >= 0 && !c->amgActive)
             CF_TRY(cluster_inner(c, order, clusterMax == 0 ? 16384 : clusterMax, &clustered));
         // opt-in: the whole loop as one cooperative kernel
-        if (!clustered && useGraph && spmv_default(c))
+        if (!clustered && useGraph && spmv_default(c) && !c->amgActive)
             CF_TRY(persistent_inner(c, kind, kind == 0 ? order : 1, persistMax, &persistent));
         if (persistent || clustered)
         {
@@ -359,6 +362,17 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
     const int n = c->n;
     const DevSell A = sell_of(c);
     std::memset(perf, 0, sizeof(*perf));
+    const bool gamg = o->preconditioner == CF_PRECOND_GAMG;
+    if (gamg && bicg)
+        return fail(CF_ERR_UNSUPPORTED, "the GAMG preconditioner is offered for cudaPCG only");
+    if (gamg && !spmv_default(c))
+        return fail(CF_ERR_UNSUPPORTED, "the GAMG preconditioner runs in the default SpMV shape");
+    // the V-cycle replaces the Chebyshev apply for this solve only
+    struct AmgScope
+    {
+        cf_context* c;
+        ~AmgScope() { c->amgActive = false; }
+    } amgScope{c};
     CF_CUDA(cudaEventRecord(c->ev2, s));
 
     // FP32 operator symmetric for PCG, as the reference stages it
@@ -407,9 +421,16 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
         perf->deflated = deflate;
         const double tc0 = wall_now();
         CF_TRY(stage_diag32(c, deflate ? 1 : 0));
+        if (gamg)
+        {
+            CF_TRY(amg_prepare(c, o->nCellsInCoarsestLevel));
+            CF_TRY(amg_stage(c, deflate ? 1 : 0, (float)o->scaleCorrection));
+            c->amgActive = true;
+        }
 
-        // Chebyshev setup (metalFoamSolver.C:224-249)
-        const int order = bicg ? 1 : o->chebyshevOrder;
+        // Chebyshev setup (metalFoamSolver.C:224-249); with GAMG the
+        // constants are the smoother's (degree nSweeps)
+        const int order = bicg ? 1 : (gamg ? o->nSweeps : o->chebyshevOrder);
         if (order < 1 || order > CF_MAX_CHEB)
             return fail(CF_ERR_INVALID_ARG, "chebyshevOrder must be in [1, 64]");
         if (order > 1)
@@ -489,6 +510,7 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
                 deflate = false;
                 perf->polished = 1;
                 CF_TRY(stage_diag32(c, 0));
+                if (gamg) CF_TRY(amg_stage(c, 0, (float)o->scaleCorrection));
                 if (o->verbose)
                     std::printf("    %s switching to exact operator (polish)\n", name);
             }
@@ -535,6 +557,15 @@ int check_options(const cf_options* o)
         return fail(CF_ERR_INVALID_ARG, "deflate must be auto, on or off");
     if (o->maxRestarts < 0) return fail(CF_ERR_INVALID_ARG, "maxRestarts must be >= 0");
     if (!(o->chebyshevRatio > 1.0)) return fail(CF_ERR_INVALID_ARG, "chebyshevRatio must be > 1");
+    if (o->preconditioner != CF_PRECOND_CHEBYSHEV && o->preconditioner != CF_PRECOND_GAMG)
+        return fail(CF_ERR_INVALID_ARG, "preconditioner must be Chebyshev or GAMG");
+    if (o->preconditioner == CF_PRECOND_GAMG &&
+        (o->nSweeps < 2 || o->nSweeps > 8 || o->nCellsInCoarsestLevel < 1 ||
+         o->nCellsInCoarsestLevel > 128 || !(o->scaleCorrection > 0.0) ||
+         !(o->scaleCorrection < 2.0)))
+        return fail(CF_ERR_INVALID_ARG, "GAMG: nSweeps must be in [2, 8], "
+                                        "nCellsInCoarsestLevel in [1, 128] and "
+                                        "scaleCorrection in (0, 2)");
     return CF_OK;
 }
 

@@ -57,6 +57,16 @@ int deflateMode(const Foam::word& w)
     return CF_DEFLATE_AUTO;
 }
 
+int preconditionerKind(const Foam::word& w)
+{
+    if (w == "Chebyshev") return CF_PRECOND_CHEBYSHEV;
+    if (w == "GAMG") return CF_PRECOND_GAMG;
+    FatalErrorInFunction
+        << "preconditioner must be Chebyshev or GAMG, not " << w
+        << Foam::exit(Foam::FatalError);
+    return CF_PRECOND_CHEBYSHEV;
+}
+
 } // anonymous namespace
 
 
@@ -200,6 +210,11 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     opts.stagnationLimit = cudaDict_.getOrDefault<label>("stagnationLimit", 0);
     opts.persistentMaxCells = cudaDict_.getOrDefault<label>("persistentMaxCells", 0);
     opts.clusterMaxCells = cudaDict_.getOrDefault<label>("clusterMaxCells", 0);
+    opts.preconditioner =
+        preconditionerKind(cudaDict_.getOrDefault<word>("preconditioner", "Chebyshev"));
+    opts.nSweeps = cudaDict_.getOrDefault<label>("nSweeps", 3);
+    opts.nCellsInCoarsestLevel = cudaDict_.getOrDefault<label>("nCellsInCoarsestLevel", 128);
+    opts.scaleCorrection = cudaDict_.getOrDefault<scalar>("scaleCorrection", 1.8);
 
     // autotune yes: time the SpMV launch shapes once per context (the mesh
     // of a context does not change during a run) and keep the fastest

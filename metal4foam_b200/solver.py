@@ -144,7 +144,19 @@ def backend_cache_clear():
 
 _CONTROL_KEYS = ("maxRestarts", "iterationsPerSync", "deflate", "chebyshevOrder",
                  "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit", "autotune",
-                 "persistentMaxCells", "clusterMaxCells")
+                 "persistentMaxCells", "clusterMaxCells", "preconditioner", "nSweeps",
+                 "nCellsInCoarsestLevel", "scaleCorrection")
+
+def _preconditioner(name) -> int:
+    """`preconditioner` of the cuda sub-dictionary: Chebyshev (the
+    reference's Chebyshev-Jacobi, default) or GAMG (aggregation multigrid
+    V-cycle, cudaPCG only)."""
+    try:
+        return _lib.PRECONDITIONERS[str(name)]
+    except KeyError:
+        raise FatalError(f"unknown preconditioner {name!r} in the cuda sub-dictionary "
+                         f"(offered: {sorted(_lib.PRECONDITIONERS)})") from None
+
 
 # backends whose SpMV launch shape has been chosen (autotune yes)
 _TUNED: Dict[tuple, dict] = {}
@@ -158,9 +170,13 @@ class cudaFoamSolver:
     ``cuda`` (``metal`` is accepted too, so existing dictionaries work)
     with ``maxRestarts``, ``iterationsPerSync``, ``deflate``,
     ``chebyshevOrder``, ``chebyshevRatio``, ``profile``, ``verbose``,
-    ``graph``, ``stagnationLimit`` and ``autotune`` (pick the SpMV launch
+    ``graph``, ``stagnationLimit``, ``autotune`` (pick the SpMV launch
     shape by timing, once per mesh and device, cached on disk; see
-    :mod:`metal4foam_b200.autotune`).
+    :mod:`metal4foam_b200.autotune`), ``persistentMaxCells``,
+    ``clusterMaxCells`` and, for cudaPCG, ``preconditioner`` (Chebyshev,
+    the reference's default, or GAMG: one aggregation multigrid V-cycle per
+    inner iteration) with ``nSweeps``, ``nCellsInCoarsestLevel`` and
+    ``scaleCorrection``.
     """
 
     typeName = "cudaFoamSolver"
@@ -209,6 +225,10 @@ class cudaFoamSolver:
             stagnationLimit=int(s.get("stagnationLimit", 0)),
             persistentMaxCells=int(s.get("persistentMaxCells", 0)),
             clusterMaxCells=int(s.get("clusterMaxCells", 0)),
+            preconditioner=_preconditioner(s.get("preconditioner", "Chebyshev")),
+            nSweeps=int(s.get("nSweeps", 3)),
+            nCellsInCoarsestLevel=int(s.get("nCellsInCoarsestLevel", 128)),
+            scaleCorrection=float(s.get("scaleCorrection", 1.8)),
         )
 
     def solveImpl(self, psi: np.ndarray, source: np.ndarray, cmpt: int = 0) -> solverPerformance:

@@ -1,0 +1,150 @@
+"""cudaPCG with the aggregation multigrid preconditioner (opt-in,
+preconditioner GAMG): the FP64 driver is the reference's, so a converged
+solve must meet the same FP64 criterion (sum|b - A psi| / normFactor below
+the tolerance, checked here in numpy) and agree with the reference
+Chebyshev-Jacobi solve of the same system to the accuracy the tolerance
+implies; the hierarchy shrinks to at most nCellsInCoarsestLevel cells;
+graph-driven and host-synchronised loops give the same bits."""
+import numpy as np
+import pytest
+
+from metal4foam_b200 import _lib, mesh
+
+pytestmark = pytest.mark.gpu
+
+PCG = _lib.CF_SOLVER_PCG
+
+
+def make_ctx(s):
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, None)
+    return ctx
+
+
+def fp64_residual(s, x, p):
+    r = s.source - mesh.amul_numpy(s, x)
+    return np.sum(np.abs(r)) / p.normFactor
+
+
+CASES = [
+    ("varcoeff_40_permuted", lambda: mesh.varcoeff3d((40, 40, 40), seed=3, permute=True), {}),
+    ("varcoeff_48x40x36", lambda: mesh.varcoeff3d((48, 40, 36), seed=4, permute=False), {}),
+    ("poisson2d_128", lambda: mesh.poisson2d(128, 128, seed=5), {}),
+    ("varcoeff_30_no_deflation", lambda: mesh.varcoeff3d((30, 28, 26), seed=6, permute=True),
+     {"deflate": "off"}),
+    ("varcoeff_36_degree3", lambda: mesh.varcoeff3d((36, 34, 32), seed=7, permute=True),
+     {"nSweeps": 3, "nCellsInCoarsestLevel": 40, "scaleCorrection": 1.6}),
+]
+
+
+@pytest.mark.parametrize("name,make,kw", CASES, ids=[c[0] for c in CASES])
+def test_gamg_converges(require_gpu, name, make, kw):
+    s = make()
+    ctx = make_ctx(s)
+    tol = 1e-7
+    xg = np.zeros(s.n)
+    pg = ctx.solve(PCG, xg, s.source,
+                   _lib.default_options(tolerance=tol, maxIter=5000, preconditioner="GAMG", **kw))
+    levels = ctx.gamg_levels()
+    xc = np.zeros(s.n)
+    pc = ctx.solve(PCG, xc, s.source, _lib.default_options(tolerance=tol, maxIter=5000,
+                                                           **{k: v for k, v in kw.items()
+                                                              if k == "deflate"}))
+    ctx.close()
+    assert pg.converged and pg.finalResidual < tol, (name, pg.finalResidual)
+    res = fp64_residual(s, xg, pg)
+    assert res == pytest.approx(pg.finalResidual, rel=1e-6, abs=1e-15)
+    assert res < tol
+    # the same system solved both ways: the solutions agree to the accuracy
+    # the residual tolerance implies
+    scale = np.max(np.abs(xc)) + 1e-30
+    assert np.max(np.abs(xg - xc)) / scale < 1e-3, name
+    assert pg.nIterations < 5000 and pc.converged
+    cap = kw.get("nCellsInCoarsestLevel", 128)
+    assert levels[0] == s.n and len(levels) >= 2 and levels[-1] <= cap
+    assert all(b < a for a, b in zip(levels, levels[1:])), levels
+
+
+def test_gamg_graph_and_host_sync_bitwise(require_gpu):
+    s = mesh.varcoeff3d((32, 30, 28), seed=8, permute=True)
+    ctx = make_ctx(s)
+    out = []
+    for graph in (1, 0, 1):
+        x = np.zeros(s.n)
+        p = ctx.solve(PCG, x, s.source, _lib.default_options(tolerance=1e-8, graph=graph,
+                                                             preconditioner="GAMG"))
+        out.append((x, p.nIterations, p.finalResidual, p.nRestarts))
+    ctx.close()
+    for x, *rest in out[1:]:
+        assert np.array_equal(x, out[0][0]) and rest == list(out[0][1:])
+
+
+def test_gamg_follows_topology_and_coefficient_changes(require_gpu):
+    """A new mesh with the same cell count rebuilds the hierarchy; new
+    coefficients on the same mesh are restaged (no stale coarse levels)."""
+    s1 = mesh.varcoeff3d((20, 20, 20), seed=9, permute=True)
+    s2 = mesh.varcoeff3d((40, 20, 10), seed=10, permute=True)
+    s3 = mesh.varcoeff3d((40, 20, 10), seed=11, permute=True)   # same mesh, other values
+    assert s1.n == s2.n
+    opts = _lib.default_options(tolerance=1e-8, preconditioner="GAMG")
+    ctx = make_ctx(s1)
+    x = np.zeros(s1.n)
+    assert ctx.solve(PCG, x, s1.source, opts).converged
+    l1 = ctx.gamg_levels()
+    for s in (s2, s3):
+        a = s.addr
+        ctx.set_topology(a.n, a.nf, *a.arrays())
+        ctx.set_coeffs(s.diag, s.upper, None)
+        x = np.zeros(s.n)
+        p = ctx.solve(PCG, x, s.source, opts)
+        assert p.converged and fp64_residual(s, x, p) < 1e-8
+        ref = make_ctx(s)
+        xr = np.zeros(s.n)
+        pr = ref.solve(PCG, xr, s.source, opts)
+        ref.close()
+        assert np.array_equal(x, xr) and p.nIterations == pr.nIterations
+    assert ctx.gamg_levels() != l1 or s2.nf != s1.nf
+    ctx.close()
+
+
+def test_gamg_rejects(require_gpu):
+    s = mesh.upwind3d((10, 9, 8), seed=12)
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, s.lower)
+    with pytest.raises(_lib.CudaFoamError) as ei:
+        ctx.solve(_lib.CF_SOLVER_PBICGSTAB, np.zeros(s.n), s.source,
+                  _lib.default_options(preconditioner="GAMG"))
+    assert ei.value.code == 8
+    for bad in (dict(nSweeps=1), dict(nSweeps=9), dict(nCellsInCoarsestLevel=0),
+                dict(nCellsInCoarsestLevel=129), dict(preconditioner=7),
+                dict(scaleCorrection=0.0), dict(scaleCorrection=2.0)):
+        kw = dict(preconditioner="GAMG")
+        kw.update(bad)
+        with pytest.raises(_lib.CudaFoamError) as ei:
+            ctx.solve(PCG, np.zeros(s.n), s.source, _lib.default_options(**kw))
+        assert ei.value.code == 1, bad
+    ctx.set_spmv_config(layout="ldu", rowsPerWarp=8, blockSize=128)
+    with pytest.raises(_lib.CudaFoamError) as ei:
+        ctx.solve(PCG, np.zeros(s.n), s.source, _lib.default_options(preconditioner="GAMG"))
+    assert ei.value.code == 8
+    assert ctx.gamg_levels() == []
+    ctx.close()
+
+
+def test_gamg_solver_surface(require_gpu):
+    from metal4foam_b200.solver import FatalError, backend_cache_clear, cudaPCG, lduMatrix
+    s = mesh.varcoeff3d((24, 22, 20), seed=13, permute=True)
+    m = lduMatrix(s.addr, s.diag, s.upper)
+    ctl = {"solver": "cudaPCG", "tolerance": 1e-7,
+           "cuda": {"preconditioner": "GAMG", "nSweeps": 2, "nCellsInCoarsestLevel": 64}}
+    x = np.zeros(s.n)
+    p = cudaPCG("p", m, ctl).solve(x, s.source)
+    assert p.converged and fp64_residual(s, x, p) < 1e-7
+    with pytest.raises(FatalError):
+        cudaPCG("p", m, {"solver": "cudaPCG", "cuda": {"preconditioner": "DIC"}}).solve(
+            np.zeros(s.n), s.source)
+    backend_cache_clear()
