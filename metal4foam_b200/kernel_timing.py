@@ -18,6 +18,10 @@ with conditional nodes); prints the solve time and iterations.
 
 --multi: one 3-component cudaPBiCGStab solve of the upwind momentum matrix
 (default 64^3) with graph 0, for the same reason.
+
+--gamg: two cudaPCG solves of the pressure matrix (default 128^3) with the
+multigrid preconditioner (preconditioner GAMG, defaults), graph 0 -- the
+first builds the hierarchy; the second is the one to profile.
 """
 from __future__ import annotations
 
@@ -78,10 +82,31 @@ def multi(dims):
     ctx.close()
 
 
+def gamg(dims):
+    s = mesh.varcoeff3d(dims, seed=1, permute=True)
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, None)
+    opts = _lib.default_options(preconditioner="GAMG", graph=0)
+    for k in range(2):
+        psi = np.zeros(s.n)
+        t0 = time.perf_counter()
+        p = ctx.solve(_lib.CF_SOLVER_PCG, psi, s.source, opts)
+        dt = time.perf_counter() - t0
+        print(f"GAMG solve {k} {dims}: {dt * 1e3:.1f} ms (host-synchronised loop), iterations "
+              f"{p.nIterations}, final residual {p.finalResidual:.3e}, levels "
+              f"{ctx.gamg_levels()}", flush=True)
+    ctx.close()
+
+
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
     if argv and argv[0] == "--batched":
         batched(int(argv[1]) if len(argv) > 1 else 48)
+        return
+    if argv and argv[0] == "--gamg":
+        gamg(tuple(int(x) for x in (argv[1] if len(argv) > 1 else "128,128,128").split(",")))
         return
     if argv and argv[0] == "--multi":
         multi(tuple(int(x) for x in (argv[1] if len(argv) > 1 else "64,64,64").split(",")))
