@@ -111,7 +111,6 @@ struct AmgData
     std::vector<AmgLevel> lv;
     std::vector<void*> allocs;
     double* coarseInv = nullptr;   // [nc * nc] inverse of the coarsest operator (row-major)
-    double* coarseWork = nullptr;  // [nc * nc] inversion workspace
     float* scale = nullptr;        // scaleCorrection of the current solve
     float hostScale = 1.0f;        // its host copy (source of the async upload)
 };
@@ -259,24 +258,24 @@ __global__ void ka_stage_vals(long long nnzp, const int* __restrict__ eface,
     }
 }
 
-// dense coarsest operator (+ s 11^T when it is singular by construction),
-// then its inverse by Gauss-Jordan without pivoting (SPD), one block
+// Dense coarsest operator (+ s 11^T when it is singular by construction)
+// and its inverse, one block: the matrix lives in shared memory and is
+// inverted in place by Gauss-Jordan without pivoting (SPD), then written out.
 __global__ void __launch_bounds__(AMG_INV_THREADS)
     ka_coarse_invert(int nc, const int* __restrict__ sliceOff, const int* __restrict__ col,
                      const int* __restrict__ eface, const double* __restrict__ upper,
-                     const double* __restrict__ diag, int shift, double* __restrict__ M,
-                     double* __restrict__ inv)
+                     const double* __restrict__ diag, int shift, double* __restrict__ inv)
 {
+    extern __shared__ double sm[];
+    double* M = sm;               // nc * nc
+    double* colp = sm + nc * nc;  // column p of the current step
     const int t = threadIdx.x;
-    for (int k = t; k < nc * nc; k += blockDim.x)
-    {
-        M[k] = 0.0;
-        inv[k] = ((k / nc) == (k % nc)) ? 1.0 : 0.0;
-    }
-    __syncthreads();
+    const int nn = nc * nc;
     double dsum = 0.0;
     for (int i = 0; i < nc; ++i) dsum += diag[i];
     const double s = shift ? dsum / ((double)nc * (double)nc) : 0.0;
+    for (int k = t; k < nn; k += blockDim.x) M[k] = s;
+    __syncthreads();
     for (int i = t; i < nc; i += blockDim.x)
     {
         M[i * nc + i] += diag[i];
@@ -291,49 +290,43 @@ __global__ void __launch_bounds__(AMG_INV_THREADS)
         }
     }
     __syncthreads();
-    if (shift)
-    {
-        for (int k = t; k < nc * nc; k += blockDim.x) M[k] += s;
-        __syncthreads();
-    }
     for (int p = 0; p < nc; ++p)
     {
-        const double piv = M[p * nc + p];
+        const double pinv = 1.0 / M[p * nc + p];
+        for (int i = t; i < nc; i += blockDim.x) colp[i] = M[i * nc + p];
         __syncthreads();
         for (int j = t; j < nc; j += blockDim.x)
-        {
-            M[p * nc + j] /= piv;
-            inv[p * nc + j] /= piv;
-        }
+            M[p * nc + j] = (j == p) ? pinv : M[p * nc + j] * pinv;
         __syncthreads();
-        for (int k = t; k < nc * nc; k += blockDim.x)
+        for (int k = t; k < nn; k += blockDim.x)
         {
             const int i = k / nc;
-            const int j = k % nc;
             if (i == p) continue;
-            const double f = M[i * nc + p];
-            if (j != p) M[k] -= f * M[p * nc + j];
-            inv[k] -= f * inv[p * nc + j];
+            const int j = k - i * nc;
+            M[k] = ((j == p) ? 0.0 : M[k]) - M[p * nc + j] * colp[i];
         }
         __syncthreads();
-        for (int i = t; i < nc; i += blockDim.x)
-            if (i != p) M[i * nc + p] = 0.0;
-        __syncthreads();
     }
+    for (int k = t; k < nn; k += blockDim.x) inv[k] = M[k];
 }
 
-// x = inv b on the coarsest level (one block)
+// x = inv b on the coarsest level (one block, a warp per row: coalesced
+// loads of the row, fixed shuffle tree)
 __global__ void __launch_bounds__(NT) ka_coarse_solve(int nc, const double* __restrict__ inv,
                                                       const float* __restrict__ b,
                                                       float* __restrict__ x,
                                                       const InnerState* st)
 {
     if (st->done) return;
-    for (int i = threadIdx.x; i < nc; i += NT)
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int i = warp; i < nc; i += NT / 32)
     {
         double s = 0.0;
-        for (int j = 0; j < nc; ++j) s += inv[i * nc + j] * (double)b[j];
-        x[i] = (float)s;
+        for (int j = lane; j < nc; j += 32) s += inv[i * nc + j] * (double)b[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) x[i] = (float)s;
     }
 }
 
@@ -372,6 +365,53 @@ __device__ __forceinline__ float row_coarse(const DevSell& A, int row, float acc
         for (int k = 0; k < 8; ++k)
             if (c[k] != -1) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
     }
+    return acc;
+}
+
+// Off-diagonal part of a coarse row, formed by T lanes together: lane
+// `sub` takes entries sub, sub + T, ... (up to four loads in flight), the
+// T partial sums are combined by a fixed shuffle tree.  Every lane of the
+// warp must call it (rows past the end pass valid = false).
+template <int T, class XF>
+__device__ __forceinline__ float row_coarse_lanes(const DevSell& A, int row, bool valid, int sub,
+                                                  XF xf)
+{
+    float acc = 0.0f;
+    if (valid)
+    {
+        const int sl = row >> 5;
+        const int b0 = A.ellW ? sl * SLICE * A.ellW : __ldg(A.sliceOff + sl);
+        const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + sl + 1) - b0) >> 5;
+        const int base = b0 + (row & 31);
+        for (int k0 = sub; k0 < w; k0 += 4 * T)
+        {
+            int c[4];
+            float v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int k = k0 + q * T;
+                if (k < w)
+                {
+                    c[q] = __ldcs(A.col + base + SLICE * k);
+                    v[q] = __ldcs(A.val + base + SLICE * k);
+                }
+                else
+                {
+                    c[q] = -1;
+                    v[q] = 0.0f;
+                }
+            }
+            float x[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = (c[q] != -1) ? xf(col_index(c[q])) : 0.0f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (c[q] != -1) acc = __fadd_rn(acc, __fmul_rn(v[q], x[q]));
+        }
+    }
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) acc = __fadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
     return acc;
 }
 
@@ -440,6 +480,52 @@ __global__ void __launch_bounds__(NT) ka_resid(DevSell A, const float* __restric
     }
 }
 
+// The coarse-level step and residual with LANES lanes per row (levels of
+// fewer than AMG_LANES_ROWS cells, where one thread per row is latency-bound).
+constexpr int AMG_LANES = 8;
+constexpr int AMG_LANES_ROWS = 100000;
+
+template <bool RESID>
+__global__ void __launch_bounds__(NT) ka_step_lanes(DevSell A, const float* __restrict__ diag,
+                                                    const float* __restrict__ rD,
+                                                    const float* __restrict__ b, const float* xin,
+                                                    float* w, float* xout,
+                                                    const float* __restrict__ cc, int j,
+                                                    const InnerState* st)
+{
+    if (st->done) return;
+    constexpr int T = AMG_LANES;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (T - 1);
+    const int warpG = (blockIdx.x * NT + threadIdx.x) >> 5;
+    const int warps = gridDim.x * (NT / 32);
+    const float c2 = j > 0 ? cc[2 * j - 1] : 0.0f;
+    const float c3 = j > 0 ? cc[2 * j] : cc[0];
+    for (int r0 = warpG * (32 / T); r0 < A.n; r0 += warps * (32 / T))
+    {
+        const int row = r0 + lane / T;
+        const bool valid = row < A.n;
+        const float off = row_coarse_lanes<T>(A, row, valid, sub,
+                                              [&](int q) { return __ldg(xin + q); });
+        if (valid && sub == 0)
+        {
+            const float xr = xin[row];
+            const float v = __fadd_rn(__fmul_rn(diag[row], xr), off);
+            if (RESID)
+            {
+                xout[row] = __fsub_rn(b[row], v);   // r = b - A x
+            }
+            else
+            {
+                const float s = __fmul_rn(__fmul_rn(c3, rD[row]), __fsub_rn(b[row], v));
+                const float wn = j > 0 ? __fadd_rn(__fmul_rn(c2, w[row]), s) : s;
+                w[row] = wn;
+                xout[row] = __fadd_rn(xr, wn);
+            }
+        }
+    }
+}
+
 // b' = P^T r: per aggregate, the sum of its rows in ascending order
 __global__ void __launch_bounds__(NT) ka_restrict(int nagg, const int* __restrict__ aggStart,
                                                   const int* __restrict__ aggRows,
@@ -492,16 +578,26 @@ int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
     AMG_LAUNCH();
     float* xa = L.x0;
     float* xb = L.x1;
+    const bool lanes = L.n < AMG_LANES_ROWS;
+    const long long laneWork = (long long)L.n * AMG_LANES;
     for (int j = 1; j < degree; ++j)
     {
-        ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
-            L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
+        if (lanes)
+            ka_step_lanes<false><<<grid_n(c, (const void*)ka_step_lanes<false>, laneWork), NT, 0,
+                                   s>>>(L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
+        else
+            ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
+                L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
         AMG_LAUNCH();
         std::swap(xa, xb);
     }
     // coarse-grid correction
-    ka_resid<MW, true><<<grid_n(c, (const void*)ka_resid<MW, true>, L.n), NT, 0, s>>>(
-        L.A, L.diag32, L.b, xa, L.r, st);
+    if (lanes)
+        ka_step_lanes<true><<<grid_n(c, (const void*)ka_step_lanes<true>, laneWork), NT, 0, s>>>(
+            L.A, L.diag32, L.rD32, L.b, xa, nullptr, L.r, cc, 0, st);
+    else
+        ka_resid<MW, true><<<grid_n(c, (const void*)ka_resid<MW, true>, L.n), NT, 0, s>>>(
+            L.A, L.diag32, L.b, xa, L.r, st);
     AMG_LAUNCH();
     AmgLevel& N = d->lv[l + 1];
     ka_restrict<<<grid_n(c, (const void*)ka_restrict, L.nagg), NT, 0, s>>>(L.nagg, L.aggStart,
@@ -515,8 +611,12 @@ int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
     // post-smoothing from x
     for (int j = 0; j < degree; ++j)
     {
-        ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
-            L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
+        if (lanes)
+            ka_step_lanes<false><<<grid_n(c, (const void*)ka_step_lanes<false>, laneWork), NT, 0,
+                                   s>>>(L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
+        else
+            ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
+                L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
         AMG_LAUNCH();
         std::swap(xa, xb);
     }
@@ -709,7 +809,6 @@ int amg_prepare(cf_context* c, int coarsestCap)
     }
     AMG_TRY(amg_alloc(c, d, &d->scale, 1));
     AMG_TRY(amg_alloc(c, d, &d->coarseInv, (size_t)Z.n * Z.n));
-    AMG_TRY(amg_alloc(c, d, &d->coarseWork, (size_t)Z.n * Z.n));
     AMG_CUDA(cudaStreamSynchronize(c->stream));
     return CF_OK;
 }
@@ -741,9 +840,12 @@ int amg_stage(cf_context* c, int deflate, float scaleCorrection)
         AMG_LAUNCH();
     }
     AmgLevel& Z = d->lv.back();
-    ka_coarse_invert<<<1, AMG_INV_THREADS, 0, s>>>(Z.n, Z.A.sliceOff, Z.A.col, Z.eface, Z.upper64,
-                                                   Z.diag64, deflate ? 1 : 0, d->coarseWork,
-                                                   d->coarseInv);
+    const int smem = (Z.n * Z.n + Z.n) * (int)sizeof(double);
+    AMG_CUDA(cudaFuncSetAttribute(ka_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem));
+    ka_coarse_invert<<<1, AMG_INV_THREADS, smem, s>>>(Z.n, Z.A.sliceOff, Z.A.col, Z.eface,
+                                                      Z.upper64, Z.diag64, deflate ? 1 : 0,
+                                                      d->coarseInv);
     AMG_LAUNCH();
     return CF_OK;
 }
