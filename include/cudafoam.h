@@ -444,6 +444,14 @@ int cf_autotune(cf_context* ctx, int32_t reps, int32_t apply, cf_spmv_config* be
  * is the mesh): *levels receives the number of levels (0 before any GAMG
  * solve), cells[0..min(levels, capacity)-1] their sizes. */
 int cf_gamg_levels(cf_context* ctx, int32_t* cells, int32_t capacity, int32_t* levels);
+/* Level `level` (>= 1) of that hierarchy as an LDU matrix, for inspection:
+ * *nFaces its faces; agg[i] (cells of level - 1; for level 1 indexed by the
+ * caller's cell numbering) the cell of `level` that cell i belongs to;
+ * diag[cells(level)], upper[nFaces] the Galerkin operator P^T A P as the
+ * last GAMG solve staged it (FP64); lowerAddr/upperAddr[nFaces] its faces
+ * (owner < neighbour, sorted).  Any array may be NULL (only *nFaces then). */
+int cf_gamg_export(cf_context* ctx, int32_t level, int32_t* nFaces, int32_t* agg, double* diag,
+                   double* upper, int32_t* lowerAddr, int32_t* upperAddr);
 
 /* ------------------------------------------------------------ no allocation */
 

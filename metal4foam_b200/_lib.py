@@ -129,6 +129,7 @@ SIGNATURES = [
     ("cf_autotune", C.c_int, [vp, i32, i32, C.POINTER(SpmvConfig), C.POINTER(TuneEntry), i32,
                               C.POINTER(i32)]),
     ("cf_gamg_levels", C.c_int, [vp, C.POINTER(i32), i32, C.POINTER(i32)]),
+    ("cf_gamg_export", C.c_int, [vp, i32, C.POINTER(i32), vp, vp, vp, vp, vp]),
     ("cf_solve_multi", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
                                  C.POINTER(Performance)]),
     ("cf_solve_multi_device", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
@@ -394,6 +395,22 @@ class Context:
         nl = C.c_int32()
         check(load().cf_gamg_levels(self.h, cells, 32, C.byref(nl)))
         return [cells[i] for i in range(min(nl.value, 32))]
+
+    def gamg_export(self, level):
+        """Level `level` (>= 1) of the GAMG hierarchy: (agg of the finer
+        level's cells, diag, upper, lowerAddr, upperAddr)."""
+        cells = self.gamg_levels()
+        nf = C.c_int32()
+        check(load().cf_gamg_export(self.h, int(level), C.byref(nf), None, None, None, None,
+                                    None))
+        agg = np.empty(cells[level - 1], np.int32)
+        diag = np.empty(cells[level], np.float64)
+        upper = np.empty(nf.value, np.float64)
+        lo = np.empty(nf.value, np.int32)
+        up = np.empty(nf.value, np.int32)
+        check(load().cf_gamg_export(self.h, int(level), C.byref(nf), ptr(agg), ptr(diag),
+                                    ptr(upper), ptr(lo), ptr(up)))
+        return agg, diag, upper, lo, up
 
     def autotune(self, reps=20, apply=True):
         """Times every SpMV launch shape on this matrix; returns (best

@@ -103,6 +103,9 @@ struct AmgLevel
     int* cfList = nullptr;
     int* intStart = nullptr;    // [nagg + 1] this level's faces inside each aggregate
     int* intList = nullptr;
+    // host copies for cf_gamg_export: this level's faces (levels >= 1) and
+    // the aggregate of each row (levels with a coarser one)
+    std::vector<int> hLow, hUpp, hAgg;
 };
 
 struct AmgData
@@ -738,6 +741,7 @@ int amg_prepare(cf_context* c, int coarsestCap)
 
         AmgLevel& L = d->lv[cur];
         L.nagg = nagg;
+        L.hAgg = agg;
         AMG_TRY(amg_upload(c, d, &L.agg, agg));
         AMG_TRY(amg_upload(c, d, &L.aggStart, aggStart));
         AMG_TRY(amg_upload(c, d, &L.aggRows, aggRows));
@@ -769,6 +773,8 @@ int amg_prepare(cf_context* c, int coarsestCap)
         AmgLevel& C = d->lv.back();
         C.n = nagg;
         C.nf = nfc;
+        C.hLow = clo;
+        C.hUpp = cup;
         C.nnzp = H.nnzp;
         int* sliceOff = nullptr;
         int* col = nullptr;
@@ -936,5 +942,36 @@ extern "C" int cf_gamg_levels(cf_context* c, int32_t* cells, int32_t capacity, i
     const int L = amg_levels(c);
     *levels = L;
     for (int l = 0; l < L && l < capacity; ++l) cells[l] = amg_level_cells(c, l);
+    return CF_OK;
+}
+
+extern "C" int cf_gamg_export(cf_context* c, int32_t level, int32_t* nFaces, int32_t* agg,
+                              double* diag, double* upper, int32_t* lowerAddr,
+                              int32_t* upperAddr)
+{
+    if (!c || !nFaces) return fail(CF_ERR_INVALID_ARG, "NULL argument");
+    AmgData* d = static_cast<AmgData*>(c->amg);
+    if (!d || level < 1 || level >= (int)d->lv.size())
+        return fail(CF_ERR_INVALID_ARG, "no such GAMG level (run a GAMG solve first)");
+    const AmgLevel& F = d->lv[level - 1];
+    const AmgLevel& L = d->lv[level];
+    *nFaces = L.nf;
+    if (agg)
+    {
+        if (level == 1)
+            for (int r = 0; r < F.n; ++r) agg[c->perm[r]] = F.hAgg[r];
+        else
+            std::copy(F.hAgg.begin(), F.hAgg.end(), agg);
+    }
+    if (lowerAddr) std::copy(L.hLow.begin(), L.hLow.end(), lowerAddr);
+    if (upperAddr) std::copy(L.hUpp.begin(), L.hUpp.end(), upperAddr);
+    cudaError_t e = cudaSuccess;
+    if (diag && e == cudaSuccess)
+        e = cudaMemcpyAsync(diag, L.diag64, sizeof(double) * L.n, cudaMemcpyDeviceToHost, c->stream);
+    if (upper && L.nf > 0 && e == cudaSuccess)
+        e = cudaMemcpyAsync(upper, L.upper64, sizeof(double) * L.nf, cudaMemcpyDeviceToHost,
+                            c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return fail(CF_ERR_CUDA, std::string("cf_gamg_export: ") + cudaGetErrorString(e));
     return CF_OK;
 }

@@ -148,3 +148,70 @@ def test_gamg_solver_surface(require_gpu):
         cudaPCG("p", m, {"solver": "cudaPCG", "cuda": {"preconditioner": "DIC"}}).solve(
             np.zeros(s.n), s.source)
     backend_cache_clear()
+
+
+def dense_ldu(n, diag, upper, lo, up):
+    A = np.diag(np.asarray(diag, np.float64)).copy()
+    A[lo, up] += upper
+    A[up, lo] += upper
+    return A
+
+
+@pytest.mark.parametrize("deflate", ["off", "on"])
+def test_gamg_galerkin_operators(require_gpu, deflate):
+    """Every coarse level is P^T A P of the level above (P the piecewise
+    constant prolongation of the exported aggregates; A - diag(A 1) on
+    level 0 when deflating), its faces in LDU order, every aggregate a
+    connected set of cells."""
+    s = mesh.varcoeff3d((14, 12, 10), seed=14, permute=True)
+    ctx = make_ctx(s)
+    x = np.zeros(s.n)
+    p = ctx.solve(PCG, x, s.source, _lib.default_options(
+        tolerance=1e-8, preconditioner="GAMG", nCellsInCoarsestLevel=8, deflate=deflate))
+    assert p.converged
+    assert bool(p.deflated) == (deflate == "on")
+    levels = ctx.gamg_levels()
+    assert len(levels) >= 3 and levels[-1] <= 8
+    a = s.addr
+    A = dense_ldu(s.n, s.diag, s.upper, a.lowerAddr, a.upperAddr)
+    if deflate == "on" and not p.polished:   # a polish restages the exact operator
+        A = A - np.diag(A.sum(axis=1))
+    lo_f, up_f = np.asarray(a.lowerAddr), np.asarray(a.upperAddr)
+    for lvl in range(1, len(levels)):
+        agg, diag, upper, lo, up = ctx.gamg_export(lvl)
+        nfine, ncoarse = levels[lvl - 1], levels[lvl]
+        assert agg.shape == (nfine,) and agg.min() == 0 and agg.max() == ncoarse - 1
+        assert np.all(np.bincount(agg, minlength=ncoarse) > 0)
+        P = np.zeros((nfine, ncoarse))
+        P[np.arange(nfine), agg] = 1.0
+        Ac_ref = P.T @ A @ P
+        Ac = dense_ldu(ncoarse, diag, upper, lo, up)
+        scale = np.max(np.abs(Ac_ref))
+        assert np.max(np.abs(Ac - Ac_ref)) <= 1e-12 * scale, lvl
+        # faces: owner < neighbour, sorted by owner then neighbour, no duplicates
+        assert np.all(lo < up)
+        key = lo.astype(np.int64) * ncoarse + up
+        assert np.all(np.diff(key) > 0)
+        # aggregates are connected through the finer level's faces
+        adj = [[] for _ in range(nfine)]
+        for f_lo, f_up in zip(lo_f, up_f):
+            if agg[f_lo] == agg[f_up]:
+                adj[f_lo].append(f_up)
+                adj[f_up].append(f_lo)
+        seen = np.zeros(nfine, bool)
+        comps = 0
+        for i in range(nfine):
+            if seen[i]:
+                continue
+            comps += 1
+            stack = [i]
+            seen[i] = True
+            while stack:
+                u = stack.pop()
+                for v in adj[u]:
+                    if not seen[v]:
+                        seen[v] = True
+                        stack.append(v)
+        assert comps == ncoarse, lvl
+        A, lo_f, up_f = Ac, lo, up
+    ctx.close()
