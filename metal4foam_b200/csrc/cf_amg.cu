@@ -315,15 +315,14 @@ __global__ void __launch_bounds__(AMG_INV_THREADS)
 
 // x = inv b on the coarsest level (one block, a warp per row: coalesced
 // loads of the row, fixed shuffle tree)
-__global__ void __launch_bounds__(NT) ka_coarse_solve(int nc, const double* __restrict__ inv,
-                                                      const float* __restrict__ b,
-                                                      float* __restrict__ x,
-                                                      const InnerState* st)
+__global__ void __launch_bounds__(AMG_INV_THREADS)
+    ka_coarse_solve(int nc, const double* __restrict__ inv, const float* __restrict__ b,
+                    float* __restrict__ x, const InnerState* st)
 {
     if (st->done) return;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    for (int i = warp; i < nc; i += NT / 32)
+    for (int i = warp; i < nc; i += AMG_INV_THREADS / 32)
     {
         double s = 0.0;
         for (int j = lane; j < nc; j += 32) s += inv[i * nc + j] * (double)b[j];
@@ -570,7 +569,7 @@ int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
     const int last = (int)d->lv.size() - 1;
     if (l == last)
     {
-        ka_coarse_solve<<<1, NT, 0, s>>>(L.n, d->coarseInv, L.b, L.x0, st);
+        ka_coarse_solve<<<1, AMG_INV_THREADS, 0, s>>>(L.n, d->coarseInv, L.b, L.x0, st);
         AMG_LAUNCH();
         *result = L.x0;
         return CF_OK;
