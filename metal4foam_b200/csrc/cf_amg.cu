@@ -332,44 +332,6 @@ __global__ void __launch_bounds__(AMG_INV_THREADS)
     }
 }
 
-// One FP32 row of a coarse level's operator (32-bit column stream; the
-// Galerkin rows hold up to ~26 entries): chunks of 8 entries whose loads
-// are independent, products added in entry order.
-template <class XF>
-__device__ __forceinline__ float row_coarse(const DevSell& A, int row, float acc, XF xf)
-{
-    const int sl = row >> 5;
-    const int b0 = A.ellW ? sl * SLICE * A.ellW : __ldg(A.sliceOff + sl);
-    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + sl + 1) - b0) >> 5;
-    const int base = b0 + (row & 31);
-    for (int k0 = 0; k0 < w; k0 += 8)
-    {
-        int c[8];
-        float v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-        {
-            if (k0 + k < w)
-            {
-                c[k] = __ldcs(A.col + base + SLICE * (k0 + k));
-                v[k] = __ldcs(A.val + base + SLICE * (k0 + k));
-            }
-            else
-            {
-                c[k] = -1;
-                v[k] = 0.0f;
-            }
-        }
-        float x[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) x[k] = (c[k] != -1) ? xf(col_index(c[k])) : 0.0f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if (c[k] != -1) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
-    }
-    return acc;
-}
-
 // Off-diagonal part of a coarse row, formed by T lanes together: lane
 // `sub` takes entries sub, sub + T, ... (up to four loads in flight), the
 // T partial sums are combined by a fixed shuffle tree.  Every lane of the
@@ -417,14 +379,6 @@ __device__ __forceinline__ float row_coarse_lanes(const DevSell& A, int row, boo
     return acc;
 }
 
-// the row of level 0 (the context's layout) or of a coarse level
-template <int MAXW, bool COARSE, class XF>
-__device__ __forceinline__ float row_level(const DevSell& A, int row, float acc, XF xf)
-{
-    if (COARSE) return row_coarse(A, row, acc, xf);
-    return row_f32<MAXW>(A, row, acc, xf);
-}
-
 // x = w = c1 rD b
 __global__ void __launch_bounds__(NT) ka_init(int n, const float* __restrict__ rD,
                                               const float* __restrict__ b,
@@ -443,7 +397,7 @@ __global__ void __launch_bounds__(NT) ka_init(int n, const float* __restrict__ r
 
 // Chebyshev step j >= 1:  w = c2 w + c3 rD (b - A xin);  xout = xin + w.
 // j = 0 starts the post-smoother from xin:  w = c1 rD (b - A xin).
-template <int MAXW, bool COARSE>
+template <int MAXW>
 __global__ void __launch_bounds__(NT) ka_step(DevSell A, const float* __restrict__ diag,
                                               const float* __restrict__ rD,
                                               const float* __restrict__ b, const float* xin,
@@ -457,8 +411,8 @@ __global__ void __launch_bounds__(NT) ka_step(DevSell A, const float* __restrict
     CF_ROWS(row, A.n)
     {
         const float xr = xin[row];
-        const float v = row_level<MAXW, COARSE>(A, row, __fmul_rn(diag[row], xr),
-                                                [&](int q) { return __ldg(xin + q); });
+        const float v = row_f32<MAXW>(A, row, __fmul_rn(diag[row], xr),
+                                      [&](int q) { return __ldg(xin + q); });
         const float s = __fmul_rn(__fmul_rn(c3, rD[row]), __fsub_rn(b[row], v));
         const float wn = j > 0 ? __fadd_rn(__fmul_rn(c2, w[row]), s) : s;
         w[row] = wn;
@@ -467,7 +421,7 @@ __global__ void __launch_bounds__(NT) ka_step(DevSell A, const float* __restrict
 }
 
 // r = b - A x
-template <int MAXW, bool COARSE>
+template <int MAXW>
 __global__ void __launch_bounds__(NT) ka_resid(DevSell A, const float* __restrict__ diag,
                                                const float* __restrict__ b,
                                                const float* __restrict__ x, float* __restrict__ r,
@@ -476,18 +430,19 @@ __global__ void __launch_bounds__(NT) ka_resid(DevSell A, const float* __restric
     if (st->done) return;
     CF_ROWS(row, A.n)
     {
-        const float v = row_level<MAXW, COARSE>(A, row, __fmul_rn(diag[row], x[row]),
-                                                [&](int q) { return __ldg(x + q); });
+        const float v = row_f32<MAXW>(A, row, __fmul_rn(diag[row], x[row]),
+                                      [&](int q) { return __ldg(x + q); });
         r[row] = __fsub_rn(b[row], v);
     }
 }
 
-// The coarse-level step and residual with LANES lanes per row (levels of
-// fewer than AMG_LANES_ROWS cells, where one thread per row is latency-bound).
-constexpr int AMG_LANES = 8;
-constexpr int AMG_LANES_ROWS = 100000;
+// The coarse-level step and residual with T lanes per row: 8 on levels of
+// fewer than AMG_LANES8_ROWS cells, where one thread per row is
+// latency-bound, 4 on larger coarse levels (both measured faster than one
+// thread per row).
+constexpr int AMG_LANES8_ROWS = 100000;
 
-template <bool RESID>
+template <bool RESID, int T>
 __global__ void __launch_bounds__(NT) ka_step_lanes(DevSell A, const float* __restrict__ diag,
                                                     const float* __restrict__ rD,
                                                     const float* __restrict__ b, const float* xin,
@@ -496,7 +451,6 @@ __global__ void __launch_bounds__(NT) ka_step_lanes(DevSell A, const float* __re
                                                     const InnerState* st)
 {
     if (st->done) return;
-    constexpr int T = AMG_LANES;
     const int lane = threadIdx.x & 31;
     const int sub = lane & (T - 1);
     const int warpG = (blockIdx.x * NT + threadIdx.x) >> 5;
@@ -559,6 +513,38 @@ constexpr int MW = MAXW_UNROLL;
 
 int grid_n(cf_context* c, const void* fn, long long n) { return grid_for(c, fn, n); }
 
+// A Chebyshev step (j; 0 starts from xin) or the residual (resid) of a
+// coarse level with the lane-parallel rows.
+int launch_lanes(cf_context* c, const AmgLevel& L, bool resid, const float* xin, float* xout, int j)
+{
+    cudaStream_t s = c->stream;
+    const InnerState* st = c->d_st;
+    const float* cc = c->d_chebC;
+    float* w = resid ? nullptr : L.w;
+    if (L.n < AMG_LANES8_ROWS)
+    {
+        const long long work = (long long)L.n * 8;
+        if (resid)
+            ka_step_lanes<true, 8><<<grid_n(c, (const void*)ka_step_lanes<true, 8>, work), NT, 0,
+                                     s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+        else
+            ka_step_lanes<false, 8><<<grid_n(c, (const void*)ka_step_lanes<false, 8>, work), NT,
+                                      0, s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+    }
+    else
+    {
+        const long long work = (long long)L.n * 4;
+        if (resid)
+            ka_step_lanes<true, 4><<<grid_n(c, (const void*)ka_step_lanes<true, 4>, work), NT, 0,
+                                     s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+        else
+            ka_step_lanes<false, 4><<<grid_n(c, (const void*)ka_step_lanes<false, 4>, work), NT,
+                                      0, s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+    }
+    AMG_LAUNCH();
+    return CF_OK;
+}
+
 // Level l >= 1 of the V-cycle on its own buffers; returns the buffer
 // holding the level's correction.
 int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
@@ -580,27 +566,13 @@ int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
     AMG_LAUNCH();
     float* xa = L.x0;
     float* xb = L.x1;
-    const bool lanes = L.n < AMG_LANES_ROWS;
-    const long long laneWork = (long long)L.n * AMG_LANES;
     for (int j = 1; j < degree; ++j)
     {
-        if (lanes)
-            ka_step_lanes<false><<<grid_n(c, (const void*)ka_step_lanes<false>, laneWork), NT, 0,
-                                   s>>>(L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
-        else
-            ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
-                L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
-        AMG_LAUNCH();
+        AMG_TRY(launch_lanes(c, L, false, xa, xb, j));
         std::swap(xa, xb);
     }
     // coarse-grid correction
-    if (lanes)
-        ka_step_lanes<true><<<grid_n(c, (const void*)ka_step_lanes<true>, laneWork), NT, 0, s>>>(
-            L.A, L.diag32, L.rD32, L.b, xa, nullptr, L.r, cc, 0, st);
-    else
-        ka_resid<MW, true><<<grid_n(c, (const void*)ka_resid<MW, true>, L.n), NT, 0, s>>>(
-            L.A, L.diag32, L.b, xa, L.r, st);
-    AMG_LAUNCH();
+    AMG_TRY(launch_lanes(c, L, true, xa, L.r, 0));
     AmgLevel& N = d->lv[l + 1];
     ka_restrict<<<grid_n(c, (const void*)ka_restrict, L.nagg), NT, 0, s>>>(L.nagg, L.aggStart,
                                                                            L.aggRows, L.r, N.b, st);
@@ -613,13 +585,7 @@ int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
     // post-smoothing from x
     for (int j = 0; j < degree; ++j)
     {
-        if (lanes)
-            ka_step_lanes<false><<<grid_n(c, (const void*)ka_step_lanes<false>, laneWork), NT, 0,
-                                   s>>>(L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
-        else
-            ka_step<MW, true><<<grid_n(c, (const void*)ka_step<MW, true>, L.n), NT, 0, s>>>(
-                L.A, L.diag32, L.rD32, L.b, xa, L.w, xb, cc, j, st);
-        AMG_LAUNCH();
+        AMG_TRY(launch_lanes(c, L, false, xa, xb, j));
         std::swap(xa, xb);
     }
     *result = xa;
@@ -881,7 +847,7 @@ int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int
     }
     float* x0 = const_cast<float*>(xa);
     // coarse-grid correction (the residual in Q, free until the p-update SpMV)
-    ka_resid<MW, false><<<grid_for(c, (const void*)ka_resid<MW, false>, c->n), NT, 0, s>>>(
+    ka_resid<MW><<<grid_for(c, (const void*)ka_resid<MW>, c->n), NT, 0, s>>>(
         A, B.diag, B.rA, x0, B.Q, c->d_st);
     AMG_LAUNCH();
     AmgLevel& L0 = d->lv[0];
@@ -896,7 +862,7 @@ int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int
     // level 0 post-smoothing; the last step forms z.r and beta
     float* xin = x0;
     float* xout = (x0 == Z[0]) ? Z[1] : Z[0];
-    ka_step<MW, false><<<grid_for(c, (const void*)ka_step<MW, false>, c->n), NT, 0, s>>>(
+    ka_step<MW><<<grid_for(c, (const void*)ka_step<MW>, c->n), NT, 0, s>>>(
         A, B.diag, B.rD, B.rA, xin, B.W1, xout, c->d_chebC, 0, c->d_st);
     AMG_LAUNCH();
     std::swap(xin, xout);
