@@ -200,23 +200,30 @@ def cpu_path_sample(sysm, precond, nthreads, budget_s):
     return (time.perf_counter() - t0) / p.nIterations, p.nIterations
 
 
-def fp64_error(sysm, psi, sec_per_iter, budget_s):
+def fp64_error(sysm, psi, sec_per_iter, budget_s, others=None):
     """Error of the GPU solution against OpenFOAM-semantics FP64 PCG
     (diagonal preconditioner, all host threads) converged to normalised
-    residual 1e-12, when about 3500 iterations fit in budget_s; else None."""
+    residual 1e-12, when about 3500 iterations fit in budget_s; else None.
+    `others` (name -> solution of the same system) are compared with the
+    same FP64 solve."""
     if psi is None or sec_per_iter * 3500 > budget_s:
         return None
     from oracle import oracle as O
     t0 = time.perf_counter()
     xr, p = O.foam_pcg(sysm, "diagonal", tolerance=1e-12, maxIter=8000,
                        nthreads=host_threads())
-    return {"rel_max_error": float(np.max(np.abs(psi - xr)) / np.max(np.abs(xr))),
-            "reference": "FP64 PCG (diagonal), normalised residual "
-                         f"{p.finalResidual:.2e} after {p.nIterations} iterations",
-            "seconds": round(time.perf_counter() - t0, 1)}
+    scale = float(np.max(np.abs(xr)))
+    out = {"rel_max_error": float(np.max(np.abs(psi - xr)) / scale),
+           "reference": "FP64 PCG (diagonal), normalised residual "
+                        f"{p.finalResidual:.2e} after {p.nIterations} iterations",
+           "seconds": round(time.perf_counter() - t0, 1)}
+    if others:
+        out["others_rel_max_error"] = {k: float(np.max(np.abs(v - xr)) / scale)
+                                       for k, v in others.items() if v is not None}
+    return out
 
 
-def cpu_baseline(sysm, budget_s, psi=None, error_budget_s=90.0):
+def cpu_baseline(sysm, budget_s, psi=None, error_budget_s=90.0, others=None):
     """Diagonal PCG on all host threads (the faster CPU configuration here)
     is the reported value; serial PCG+DIC (OpenFOAM's default, the
     reference's own comparison) is reported beside it, and the error of
@@ -226,7 +233,7 @@ def cpu_baseline(sysm, budget_s, psi=None, error_budget_s=90.0):
     sec_dic, it_dic = cpu_path_sample(sysm, "DIC", 1, min(budget_s, 8.0))
     v_diag = 1.0 / (sec_diag * CPU_ITERS["diagonal"])
     v_dic = 1.0 / (sec_dic * CPU_ITERS["DIC"])
-    err = fp64_error(sysm, psi, sec_diag, error_budget_s)
+    err = fp64_error(sysm, psi, sec_diag, error_budget_s, others)
     return {
         "gpu_error_vs_fp64": err,
         "value": round(v_diag, 6), "unit": "solves/s", "cores": nt, "kind": "port",
@@ -435,7 +442,8 @@ def run_gamg(ctx, d_diag, d_upper, d_src, stream, ms_reference, steps=5):
     step()
     ms = time_cuda(step, steps, stream) / steps
     p = perfs[-1]
-    return {"workload": "the headline system, cudaPCG preconditioner GAMG (opt-in; the "
+    psi = d_psi.cpu().numpy()
+    return psi, {"workload": "the headline system, cudaPCG preconditioner GAMG (opt-in; the "
                         "reference has no GAMG on its GPU path)",
             "options": {"nSweeps": opts.nSweeps, "scaleCorrection": opts.scaleCorrection,
                         "nCellsInCoarsestLevel": opts.nCellsInCoarsestLevel},
@@ -764,16 +772,21 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": launches,
         }
         sols = {}
+        psi_gamg = None
         if not args.no_extras:
             out["batched"] = batched
             out["adjoint"] = run_adjoint(local, stream)
             out["multi_rhs"] = run_multi_rhs(local, stream)
             out["configs"], sols = run_small_configs(local, stream)
-            out["gamg"] = run_gamg(ctx, d_diag, d_upper, d_src, stream, ms_max / args.steps)
+            psi_gamg, out["gamg"] = run_gamg(ctx, d_diag, d_upper, d_src, stream,
+                                             ms_max / args.steps)
             out["autotune"] = run_autotune_table(ctx, n, nf)
         if ws == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(sysm, args.cpu_budget, psi_out,
-                                               args.error_budget)
+                                               args.error_budget, {"gamg": psi_gamg})
+            err = out["cpu_baseline"].get("gpu_error_vs_fp64") or {}
+            if "gamg" in out and "gamg" in err.get("others_rel_max_error", {}):
+                out["gamg"]["error_vs_fp64"] = err["others_rel_max_error"]["gamg"]
             if sols:
                 out["cpu_baseline"]["configs"] = cpu_small_configs(sols, args.cpu_budget)
     ctx.close()
