@@ -8,12 +8,14 @@
 // Chebyshev-Jacobi polynomial (.C:342-385) is replaced by one symmetric
 // V-cycle, so PCG keeps a fixed SPD preconditioner.
 //
-// Hierarchy (built once per topology on the host): level 0 is the
-// context's matrix in its internal row order.  Each level's cells are
-// grouped into aggregates by root-based greedy aggregation on the cell
-// graph (a cell whose neighbours are all free becomes a root and takes
-// them; leftovers join a neighbouring aggregate); the aggregates, numbered
-// in the order their roots are met, are the next level's cells.  The
+// Hierarchy (built once per topology on the host, by the first GAMG solve):
+// level 0 is the context's matrix in its internal row order.  Each level's
+// cells are grouped into aggregates by root-based greedy aggregation along
+// the strong couplings of that solve's coefficients (a cell whose strong
+// neighbours are all free becomes a root and takes them; the others join
+// the aggregate they are most strongly coupled to); the aggregates,
+// numbered in the order their roots are met, are the next level's cells.
+// Later solves keep the hierarchy and re-sum its operators.  The
 // coarse operator is the Galerkin product P^T A P with the piecewise
 // constant P: a coarse face sums the fine faces between its two
 // aggregates, a coarse diagonal sums its cells' diagonals and twice the
@@ -36,6 +38,7 @@
 #include "cf_host.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -75,6 +78,7 @@ constexpr int AMG_MAX_COARSEST = 128;
 constexpr int AMG_MAX_LEVELS = 16;
 constexpr int AMG_INV_THREADS = 1024;
 constexpr int AMG_MAX_AGG = 8;       // cells per root aggregate at most
+constexpr double AMG_STRONG = 0.08;  // strong coupling: |a_ij| >= this * sqrt(a_ii a_jj)
 
 struct AmgLevel
 {
@@ -143,38 +147,54 @@ int amg_upload(cf_context* c, AmgData* d, T** p, const std::vector<T>& h)
     return CF_OK;
 }
 
-// Root-based greedy aggregation of an undirected graph (CSR adjacency).
-// A root takes at most AMG_MAX_AGG - 1 neighbours, so coarse levels, whose
-// graphs are denser, still coarsen by a factor of about 8 per level.
+// Root-based greedy aggregation of the cell graph (CSR adjacency) guided by
+// the coupling strength s_ij = |a_ij| / sqrt(a_ii a_jj) of each edge: a
+// cell with at least one strong edge (s_ij >= AMG_STRONG) whose strong
+// neighbours are all free becomes a root and takes its free strong
+// neighbours, at most AMG_MAX_AGG - 1 of them (so coarse levels, whose
+// graphs are denser, still coarsen by about 8 per level); every other cell
+// joins the aggregated neighbour it is most strongly coupled to.  Strong
+// edges keep cells that are tightly coupled (large coefficients) together,
+// which a piecewise constant interpolation needs on heterogeneous media.
 int aggregate(int n, const std::vector<int>& xadj, const std::vector<int>& adj,
-              std::vector<int>& agg)
+              const std::vector<double>& str, std::vector<int>& agg)
 {
     agg.assign(n, -1);
     int nagg = 0;
-    // roots: a free cell whose neighbours are all free takes (up to the cap of) them
     for (int i = 0; i < n; ++i)
     {
         if (agg[i] >= 0) continue;
         bool free = true;
-        for (int q = xadj[i]; q < xadj[i + 1] && free; ++q) free = agg[adj[q]] < 0;
-        if (!free) continue;
+        bool anyStrong = false;
+        for (int q = xadj[i]; q < xadj[i + 1] && free; ++q)
+            if (str[q] >= AMG_STRONG)
+            {
+                anyStrong = true;
+                free = agg[adj[q]] < 0;
+            }
+        if (!free || !anyStrong) continue;
         agg[i] = nagg;
         int taken = 1;
-        for (int q = xadj[i]; q < xadj[i + 1] && taken < AMG_MAX_AGG; ++q, ++taken)
-            agg[adj[q]] = nagg;
+        for (int q = xadj[i]; q < xadj[i + 1] && taken < AMG_MAX_AGG; ++q)
+            if (str[q] >= AMG_STRONG && agg[adj[q]] < 0)
+            {
+                agg[adj[q]] = nagg;
+                ++taken;
+            }
         ++nagg;
     }
-    // leftovers join the first aggregated neighbour (decided against the
-    // root phase's assignment only, so the order of the sweep does not chain)
+    // the rest join their most strongly coupled aggregated neighbour
+    // (decided against the root phase's assignment only)
     std::vector<int> join(n, -1);
     for (int i = 0; i < n; ++i)
     {
         if (agg[i] >= 0) continue;
+        double best = -1.0;
         for (int q = xadj[i]; q < xadj[i + 1]; ++q)
-            if (agg[adj[q]] >= 0)
+            if (agg[adj[q]] >= 0 && str[q] > best)
             {
+                best = str[q];
                 join[i] = agg[adj[q]];
-                break;
             }
     }
     for (int i = 0; i < n; ++i)
@@ -184,15 +204,20 @@ int aggregate(int n, const std::vector<int>& xadj, const std::vector<int>& adj,
     {
         if (agg[i] >= 0) continue;
         agg[i] = nagg;
-        for (int q = xadj[i]; q < xadj[i + 1]; ++q)
-            if (agg[adj[q]] < 0) agg[adj[q]] = nagg;
+        int taken = 1;
+        for (int q = xadj[i]; q < xadj[i + 1] && taken < AMG_MAX_AGG; ++q)
+            if (agg[adj[q]] < 0)
+            {
+                agg[adj[q]] = nagg;
+                ++taken;
+            }
         ++nagg;
     }
     return nagg;
 }
 
 void csr_of_faces(int n, const std::vector<int>& lo, const std::vector<int>& up,
-                  std::vector<int>& xadj, std::vector<int>& adj)
+                  std::vector<int>& xadj, std::vector<int>& adj, std::vector<int>& adjFace)
 {
     xadj.assign(n + 1, 0);
     for (size_t f = 0; f < lo.size(); ++f)
@@ -202,10 +227,13 @@ void csr_of_faces(int n, const std::vector<int>& lo, const std::vector<int>& up,
     }
     for (int i = 0; i < n; ++i) xadj[i + 1] += xadj[i];
     adj.assign(xadj[n], 0);
+    adjFace.assign(xadj[n], 0);
     std::vector<int> pos(xadj.begin(), xadj.end() - 1);
     for (size_t f = 0; f < lo.size(); ++f)
     {
+        adjFace[pos[lo[f]]] = (int)f;
         adj[pos[lo[f]]++] = up[f];
+        adjFace[pos[up[f]]] = (int)f;
         adj[pos[up[f]]++] = lo[f];
     }
 }
@@ -646,17 +674,36 @@ int amg_prepare(cf_context* c, int coarsestCap)
             up[f] = iperm[up[f]];
         }
     }
+    // the coefficients the aggregation is guided by: those staged for this
+    // solve (internal-order diagonal, caller-order faces); later solves with
+    // other coefficients keep the hierarchy and re-sum its operators
+    std::vector<double> hd(n), hu(nf);
+    AMG_CUDA(cudaMemcpyAsync(hd.data(), c->d_diag64, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                             c->stream));
+    if (nf > 0)
+        AMG_CUDA(cudaMemcpyAsync(hu.data(), c->d_upper, sizeof(double) * nf,
+                                 cudaMemcpyDeviceToHost, c->stream));
+    AMG_CUDA(cudaStreamSynchronize(c->stream));
     d->lv.emplace_back();
     d->lv[0].n = n;
     d->lv[0].nf = nf;
     int cur = 0;
-    while ((int)d->lv.size() < AMG_MAX_LEVELS && d->lv[cur].n > coarsestCap)
+    // (at least one coarse level, also for meshes already below the cap)
+    while ((int)d->lv.size() < AMG_MAX_LEVELS &&
+           (d->lv[cur].n > coarsestCap || d->lv.size() == 1))
     {
         const int nl = d->lv[cur].n;
         const int nfl = (int)lo.size();
-        std::vector<int> xadj, adj, agg;
-        csr_of_faces(nl, lo, up, xadj, adj);
-        const int nagg = aggregate(nl, xadj, adj, agg);
+        std::vector<int> xadj, adj, adjFace, agg;
+        csr_of_faces(nl, lo, up, xadj, adj, adjFace);
+        std::vector<double> str(adj.size());
+        for (int i = 0; i < nl; ++i)
+            for (int q = xadj[i]; q < xadj[i + 1]; ++q)
+            {
+                const double dd = std::fabs(hd[i]) * std::fabs(hd[adj[q]]);
+                str[q] = dd > 0.0 ? std::fabs(hu[adjFace[q]]) / std::sqrt(dd) : 0.0;
+            }
+        const int nagg = aggregate(nl, xadj, adj, str, agg);
         if (nagg >= nl || nagg < 1) break;   // no coarsening possible
         // members of each aggregate (ascending rows)
         std::vector<int> aggStart(nagg + 1, 0), aggRows(nl);
@@ -765,6 +812,20 @@ int amg_prepare(cf_context* c, int coarsestCap)
         AMG_TRY(amg_alloc(c, d, &C.x1, nagg));
         AMG_TRY(amg_alloc(c, d, &C.w, nagg));
         AMG_TRY(amg_alloc(c, d, &C.r, nagg));
+        // the coarse level's coefficients on the host (the same Galerkin sums
+        // the device forms for every solve), for the next aggregation
+        {
+            std::vector<double> cd(nagg, 0.0), cu(nfc, 0.0);
+            for (int k = 0; k < nagg; ++k)
+            {
+                for (int q = aggStart[k]; q < aggStart[k + 1]; ++q) cd[k] += hd[aggRows[q]];
+                for (int q = intStart[k]; q < intStart[k + 1]; ++q) cd[k] += 2.0 * hu[intList[q]];
+            }
+            for (int F = 0; F < nfc; ++F)
+                for (int q = cfStart[F]; q < cfStart[F + 1]; ++q) cu[F] += hu[cfList[q]];
+            hd.swap(cd);
+            hu.swap(cu);
+        }
         lo.swap(clo);
         up.swap(cup);
         cur = (int)d->lv.size() - 1;
