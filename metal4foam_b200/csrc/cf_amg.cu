@@ -79,6 +79,7 @@ constexpr int AMG_MAX_LEVELS = 16;
 constexpr int AMG_INV_THREADS = 1024;
 constexpr int AMG_MAX_AGG = 8;       // cells per root aggregate at most
 constexpr double AMG_STRONG = 0.08;  // strong coupling: |a_ij| >= this * sqrt(a_ii a_jj)
+constexpr int AMG_COARSE_DEGREE = 2; // smoother degree below level 0 (at most nSweeps)
 
 struct AmgLevel
 {
@@ -466,8 +467,8 @@ __global__ void __launch_bounds__(NT) ka_resid(DevSell A, const float* __restric
 
 // The coarse-level step and residual with T lanes per row: 8 on levels of
 // fewer than AMG_LANES8_ROWS cells, where one thread per row is
-// latency-bound, 4 on larger coarse levels (both measured faster than one
-// thread per row).
+// latency-bound, 2 on larger coarse levels (measured faster than 1, 4 or 8
+// there).
 constexpr int AMG_LANES8_ROWS = 100000;
 
 template <bool RESID, int T>
@@ -561,12 +562,12 @@ int launch_lanes(cf_context* c, const AmgLevel& L, bool resid, const float* xin,
     }
     else
     {
-        const long long work = (long long)L.n * 4;
+        const long long work = (long long)L.n * 2;
         if (resid)
-            ka_step_lanes<true, 4><<<grid_n(c, (const void*)ka_step_lanes<true, 4>, work), NT, 0,
+            ka_step_lanes<true, 2><<<grid_n(c, (const void*)ka_step_lanes<true, 2>, work), NT, 0,
                                      s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
         else
-            ka_step_lanes<false, 4><<<grid_n(c, (const void*)ka_step_lanes<false, 4>, work), NT,
+            ka_step_lanes<false, 2><<<grid_n(c, (const void*)ka_step_lanes<false, 2>, work), NT,
                                       0, s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
     }
     AMG_LAUNCH();
@@ -916,7 +917,9 @@ int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int
         L0.nagg, L0.aggStart, L0.aggRows, B.Q, d->lv[1].b, c->d_st);
     AMG_LAUNCH();
     float* xc = nullptr;
-    AMG_TRY(vcycle_coarse(c, d, 1, degree, &xc));
+    // coarse levels smooth with degree 2: their Galerkin rows are wide, and
+    // one step less there costs fewer iterations than it saves
+    AMG_TRY(vcycle_coarse(c, d, 1, degree > AMG_COARSE_DEGREE ? AMG_COARSE_DEGREE : degree, &xc));
     ka_prolong<<<grid_for(c, (const void*)ka_prolong, c->n), NT, 0, s>>>(c->n, L0.agg, xc,
                                                                          d->scale, x0, c->d_st);
     AMG_LAUNCH();
