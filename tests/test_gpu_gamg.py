@@ -231,3 +231,27 @@ def test_gamg_galerkin_operators(require_gpu, deflate):
         assert comps == ncoarse, lvl
         A, lo_f, up_f = Ac, lo, up
     ctx.close()
+
+
+def test_gamg_with_driver_controls(require_gpu):
+    """The V-cycle body under the driver's other controls: convergence
+    tests every 4 iterations, an iteration cap that stops the solve early
+    (not converged, residual still consistent), and a minimum iteration
+    count that forces iterations past convergence."""
+    s = mesh.varcoeff3d((30, 28, 26), seed=16, permute=True)
+    ctx = make_ctx(s)
+    base = dict(tolerance=1e-8, preconditioner="GAMG")
+    x = np.zeros(s.n)
+    p = ctx.solve(PCG, x, s.source, _lib.default_options(iterationsPerSync=4, **base))
+    assert p.converged and fp64_residual(s, x, p) < 1e-8
+    x = np.zeros(s.n)
+    p = ctx.solve(PCG, x, s.source, _lib.default_options(maxIter=3, **base))
+    assert not p.converged and p.nIterations <= 3
+    assert fp64_residual(s, x, p) == pytest.approx(p.finalResidual, rel=1e-6)
+    x = np.zeros(s.n)
+    p1 = ctx.solve(PCG, x, s.source, _lib.default_options(**base))
+    x = np.zeros(s.n)
+    p2 = ctx.solve(PCG, x, s.source, _lib.default_options(minIter=p1.nIterations + 5,
+                                                          maxIter=5000, **base))
+    assert p2.converged and p2.nIterations >= p1.nIterations
+    ctx.close()
