@@ -342,22 +342,34 @@ __global__ void __launch_bounds__(AMG_INV_THREADS)
     for (int k = t; k < nn; k += blockDim.x) inv[k] = M[k];
 }
 
-// x = inv b on the coarsest level (one block, a warp per row: coalesced
-// loads of the row, fixed shuffle tree)
+// The coarsest level: b = P^T r (per aggregate, its rows in ascending
+// order) and x = inv b, one block (a warp per row of the GEMV: coalesced
+// loads, fixed shuffle tree).
 __global__ void __launch_bounds__(AMG_INV_THREADS)
-    ka_coarse_solve(int nc, const double* __restrict__ inv, const float* __restrict__ b,
-                    float* __restrict__ x, const InnerState* st)
+    ka_restrict_coarse_solve(int nc, const int* __restrict__ aggStart,
+                             const int* __restrict__ aggRows, const float* __restrict__ r,
+                             const double* __restrict__ inv, float* __restrict__ b,
+                             float* __restrict__ x, const InnerState* st)
 {
+    __shared__ float sb[AMG_MAX_COARSEST];
     if (st->done) return;
+    for (int k = threadIdx.x; k < nc; k += AMG_INV_THREADS)
+    {
+        float acc = 0.0f;
+        for (int q = aggStart[k]; q < aggStart[k + 1]; ++q) acc = __fadd_rn(acc, r[aggRows[q]]);
+        sb[k] = acc;
+        b[k] = acc;
+    }
+    __syncthreads();
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     for (int i = warp; i < nc; i += AMG_INV_THREADS / 32)
     {
-        double s = 0.0;
-        for (int j = lane; j < nc; j += 32) s += inv[i * nc + j] * (double)b[j];
+        double acc = 0.0;
+        for (int j = lane; j < nc; j += 32) acc += inv[i * nc + j] * (double)sb[j];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) x[i] = (float)s;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) x[i] = (float)acc;
     }
 }
 
@@ -408,40 +420,65 @@ __device__ __forceinline__ float row_coarse_lanes(const DevSell& A, int row, boo
     return acc;
 }
 
-// x = w = c1 rD b
-__global__ void __launch_bounds__(NT) ka_init(int n, const float* __restrict__ rD,
-                                              const float* __restrict__ b,
-                                              const float* __restrict__ cc, float* __restrict__ x,
-                                              float* __restrict__ w, const InnerState* st)
+// b = P^T r (per aggregate, its rows in ascending order) and the start of
+// the level's pre-smoothing from zero, x = w = c1 rD b
+__global__ void __launch_bounds__(NT) ka_restrict_init(int n, const int* __restrict__ aggStart,
+                                                       const int* __restrict__ aggRows,
+                                                       const float* __restrict__ r,
+                                                       const float* __restrict__ rD,
+                                                       const float* __restrict__ cc,
+                                                       float* __restrict__ b, float* __restrict__ x,
+                                                       float* __restrict__ w, const InnerState* st)
 {
     if (st->done) return;
     const float c1 = cc[0];
     CF_ROWS(row, n)
     {
-        const float v = __fmul_rn(__fmul_rn(c1, rD[row]), b[row]);
+        float acc = 0.0f;
+        for (int q = aggStart[row]; q < aggStart[row + 1]; ++q) acc = __fadd_rn(acc, r[aggRows[q]]);
+        b[row] = acc;
+        const float v = __fmul_rn(__fmul_rn(c1, rD[row]), acc);
         x[row] = v;
         w[row] = v;
     }
 }
 
+// The iterate a smoothing step starts from: xin, or with PROLONG the
+// prolonged xin + a xc[agg] (the coarse-grid correction applied on the fly,
+// rounded as a separate update would be).
+template <bool PROLONG>
+struct StartX
+{
+    const float* xin;
+    const int* agg;
+    const float* xc;
+    float a;
+    __device__ __forceinline__ float operator()(int q) const
+    {
+        if (!PROLONG) return __ldg(xin + q);
+        return __fadd_rn(__ldg(xin + q), __fmul_rn(a, __ldg(xc + __ldg(agg + q))));
+    }
+};
+
 // Chebyshev step j >= 1:  w = c2 w + c3 rD (b - A xin);  xout = xin + w.
 // j = 0 starts the post-smoother from xin:  w = c1 rD (b - A xin).
-template <int MAXW>
+template <int MAXW, bool PROLONG>
 __global__ void __launch_bounds__(NT) ka_step(DevSell A, const float* __restrict__ diag,
                                               const float* __restrict__ rD,
                                               const float* __restrict__ b, const float* xin,
-                                              float* w, float* xout,
-                                              const float* __restrict__ cc, int j,
+                                              const int* __restrict__ agg, const float* xc,
+                                              const float* __restrict__ scale, float* w,
+                                              float* xout, const float* __restrict__ cc, int j,
                                               const InnerState* st)
 {
     if (st->done) return;
     const float c2 = j > 0 ? cc[2 * j - 1] : 0.0f;
     const float c3 = j > 0 ? cc[2 * j] : cc[0];
+    const StartX<PROLONG> xf{xin, agg, xc, PROLONG ? *scale : 0.0f};
     CF_ROWS(row, A.n)
     {
-        const float xr = xin[row];
-        const float v = row_f32<MAXW>(A, row, __fmul_rn(diag[row], xr),
-                                      [&](int q) { return __ldg(xin + q); });
+        const float xr = xf(row);
+        const float v = row_f32<MAXW>(A, row, __fmul_rn(diag[row], xr), xf);
         const float s = __fmul_rn(__fmul_rn(c3, rD[row]), __fsub_rn(b[row], v));
         const float wn = j > 0 ? __fadd_rn(__fmul_rn(c2, w[row]), s) : s;
         w[row] = wn;
@@ -471,13 +508,14 @@ __global__ void __launch_bounds__(NT) ka_resid(DevSell A, const float* __restric
 // there).
 constexpr int AMG_LANES8_ROWS = 100000;
 
-template <bool RESID, int T>
+template <bool RESID, int T, bool PROLONG>
 __global__ void __launch_bounds__(NT) ka_step_lanes(DevSell A, const float* __restrict__ diag,
                                                     const float* __restrict__ rD,
                                                     const float* __restrict__ b, const float* xin,
-                                                    float* w, float* xout,
-                                                    const float* __restrict__ cc, int j,
-                                                    const InnerState* st)
+                                                    const int* __restrict__ agg, const float* xc,
+                                                    const float* __restrict__ scale, float* w,
+                                                    float* xout, const float* __restrict__ cc,
+                                                    int j, const InnerState* st)
 {
     if (st->done) return;
     const int lane = threadIdx.x & 31;
@@ -486,15 +524,15 @@ __global__ void __launch_bounds__(NT) ka_step_lanes(DevSell A, const float* __re
     const int warps = gridDim.x * (NT / 32);
     const float c2 = j > 0 ? cc[2 * j - 1] : 0.0f;
     const float c3 = j > 0 ? cc[2 * j] : cc[0];
+    const StartX<PROLONG> xf{xin, agg, xc, PROLONG ? *scale : 0.0f};
     for (int r0 = warpG * (32 / T); r0 < A.n; r0 += warps * (32 / T))
     {
         const int row = r0 + lane / T;
         const bool valid = row < A.n;
-        const float off = row_coarse_lanes<T>(A, row, valid, sub,
-                                              [&](int q) { return __ldg(xin + q); });
+        const float off = row_coarse_lanes<T>(A, row, valid, sub, xf);
         if (valid && sub == 0)
         {
-            const float xr = xin[row];
+            const float xr = xf(row);
             const float v = __fadd_rn(__fmul_rn(diag[row], xr), off);
             if (RESID)
             {
@@ -511,110 +549,90 @@ __global__ void __launch_bounds__(NT) ka_step_lanes(DevSell A, const float* __re
     }
 }
 
-// b' = P^T r: per aggregate, the sum of its rows in ascending order
-__global__ void __launch_bounds__(NT) ka_restrict(int nagg, const int* __restrict__ aggStart,
-                                                  const int* __restrict__ aggRows,
-                                                  const float* __restrict__ r,
-                                                  float* __restrict__ bc, const InnerState* st)
-{
-    if (st->done) return;
-    for (int K = blockIdx.x * NT + threadIdx.x; K < nagg; K += gridDim.x * NT)
-    {
-        float s = 0.0f;
-        for (int q = aggStart[K]; q < aggStart[K + 1]; ++q) s = __fadd_rn(s, r[aggRows[q]]);
-        bc[K] = s;
-    }
-}
 
-// x += a P x' (a = scaleCorrection; a fixed factor keeps the cycle a
-// fixed symmetric operator, positive definite for 0 < a < 2)
-__global__ void __launch_bounds__(NT) ka_prolong(int n, const int* __restrict__ agg,
-                                                 const float* __restrict__ xc,
-                                                 const float* __restrict__ scale,
-                                                 float* __restrict__ x, const InnerState* st)
-{
-    if (st->done) return;
-    const float a = *scale;
-    CF_ROWS(row, n) x[row] = __fadd_rn(x[row], __fmul_rn(a, xc[agg[row]]));
-}
 
 constexpr int MW = MAXW_UNROLL;
 
 int grid_n(cf_context* c, const void* fn, long long n) { return grid_for(c, fn, n); }
 
-// A Chebyshev step (j; 0 starts from xin) or the residual (resid) of a
-// coarse level with the lane-parallel rows.
-int launch_lanes(cf_context* c, const AmgLevel& L, bool resid, const float* xin, float* xout, int j)
+// A Chebyshev step (j; 0 starts from xin, prolonged on the fly when xc is
+// given) or the residual (resid) of a coarse level with the lane-parallel
+// rows.
+int launch_lanes(cf_context* c, AmgData* d, const AmgLevel& L, bool resid, const float* xin,
+                 const float* xc, float* xout, int j)
 {
     cudaStream_t s = c->stream;
     const InnerState* st = c->d_st;
     const float* cc = c->d_chebC;
     float* w = resid ? nullptr : L.w;
+    const int* agg = L.agg;
+    const float* sc = d->scale;
+#define AMG_LANES_LAUNCH(RES, T, PRO)                                                        \
+    ka_step_lanes<RES, T, PRO><<<grid_n(c, (const void*)ka_step_lanes<RES, T, PRO>,          \
+                                        (long long)L.n * T),                                   \
+                                 NT, 0, s>>>(L.A, L.diag32, L.rD32, L.b, xin, agg, xc, sc, w, \
+                                             xout, cc, j, st)
+    const bool pro = xc != nullptr;
     if (L.n < AMG_LANES8_ROWS)
     {
-        const long long work = (long long)L.n * 8;
         if (resid)
-            ka_step_lanes<true, 8><<<grid_n(c, (const void*)ka_step_lanes<true, 8>, work), NT, 0,
-                                     s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+            AMG_LANES_LAUNCH(true, 8, false);
+        else if (pro)
+            AMG_LANES_LAUNCH(false, 8, true);
         else
-            ka_step_lanes<false, 8><<<grid_n(c, (const void*)ka_step_lanes<false, 8>, work), NT,
-                                      0, s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+            AMG_LANES_LAUNCH(false, 8, false);
     }
     else
     {
-        const long long work = (long long)L.n * 2;
         if (resid)
-            ka_step_lanes<true, 2><<<grid_n(c, (const void*)ka_step_lanes<true, 2>, work), NT, 0,
-                                     s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+            AMG_LANES_LAUNCH(true, 2, false);
+        else if (pro)
+            AMG_LANES_LAUNCH(false, 2, true);
         else
-            ka_step_lanes<false, 2><<<grid_n(c, (const void*)ka_step_lanes<false, 2>, work), NT,
-                                      0, s>>>(L.A, L.diag32, L.rD32, L.b, xin, w, xout, cc, j, st);
+            AMG_LANES_LAUNCH(false, 2, false);
     }
+#undef AMG_LANES_LAUNCH
     AMG_LAUNCH();
     return CF_OK;
 }
 
-// Level l >= 1 of the V-cycle on its own buffers; returns the buffer
-// holding the level's correction.
-int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, float** result)
+// Level l >= 1 of the V-cycle on its own buffers, from the residual rf of
+// level l - 1 (restricted here); returns the buffer holding the level's
+// correction, still to be prolonged by the caller.
+int vcycle_coarse(cf_context* c, AmgData* d, int l, int degree, const float* rf, float** result)
 {
     AmgLevel& L = d->lv[l];
+    const AmgLevel& F = d->lv[l - 1];
     cudaStream_t s = c->stream;
     const InnerState* st = c->d_st;
     const int last = (int)d->lv.size() - 1;
     if (l == last)
     {
-        ka_coarse_solve<<<1, AMG_INV_THREADS, 0, s>>>(L.n, d->coarseInv, L.b, L.x0, st);
+        ka_restrict_coarse_solve<<<1, AMG_INV_THREADS, 0, s>>>(L.n, F.aggStart, F.aggRows, rf,
+                                                               d->coarseInv, L.b, L.x0, st);
         AMG_LAUNCH();
         *result = L.x0;
         return CF_OK;
     }
-    const float* cc = c->d_chebC;
-    // pre-smoothing from zero
-    ka_init<<<grid_n(c, (const void*)ka_init, L.n), NT, 0, s>>>(L.n, L.rD32, L.b, cc, L.x0, L.w, st);
+    // right-hand side and pre-smoothing from zero
+    ka_restrict_init<<<grid_n(c, (const void*)ka_restrict_init, L.n), NT, 0, s>>>(
+        L.n, F.aggStart, F.aggRows, rf, L.rD32, c->d_chebC, L.b, L.x0, L.w, st);
     AMG_LAUNCH();
     float* xa = L.x0;
     float* xb = L.x1;
     for (int j = 1; j < degree; ++j)
     {
-        AMG_TRY(launch_lanes(c, L, false, xa, xb, j));
+        AMG_TRY(launch_lanes(c, d, L, false, xa, nullptr, xb, j));
         std::swap(xa, xb);
     }
     // coarse-grid correction
-    AMG_TRY(launch_lanes(c, L, true, xa, L.r, 0));
-    AmgLevel& N = d->lv[l + 1];
-    ka_restrict<<<grid_n(c, (const void*)ka_restrict, L.nagg), NT, 0, s>>>(L.nagg, L.aggStart,
-                                                                           L.aggRows, L.r, N.b, st);
-    AMG_LAUNCH();
+    AMG_TRY(launch_lanes(c, d, L, true, xa, nullptr, L.r, 0));
     float* xc = nullptr;
-    AMG_TRY(vcycle_coarse(c, d, l + 1, degree, &xc));
-    ka_prolong<<<grid_n(c, (const void*)ka_prolong, L.n), NT, 0, s>>>(L.n, L.agg, xc, d->scale,
-                                                                      xa, st);
-    AMG_LAUNCH();
-    // post-smoothing from x
+    AMG_TRY(vcycle_coarse(c, d, l + 1, degree, L.r, &xc));
+    // post-smoothing from x + a P x'
     for (int j = 0; j < degree; ++j)
     {
-        AMG_TRY(launch_lanes(c, L, false, xa, xb, j));
+        AMG_TRY(launch_lanes(c, d, L, false, xa, j == 0 ? xc : nullptr, xb, j));
         std::swap(xa, xb);
     }
     *result = xa;
@@ -912,22 +930,17 @@ int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int
     ka_resid<MW><<<grid_for(c, (const void*)ka_resid<MW>, c->n), NT, 0, s>>>(
         A, B.diag, B.rA, x0, B.Q, c->d_st);
     AMG_LAUNCH();
-    AmgLevel& L0 = d->lv[0];
-    ka_restrict<<<grid_for(c, (const void*)ka_restrict, L0.nagg), NT, 0, s>>>(
-        L0.nagg, L0.aggStart, L0.aggRows, B.Q, d->lv[1].b, c->d_st);
-    AMG_LAUNCH();
+    const AmgLevel& L0 = d->lv[0];
     float* xc = nullptr;
     // coarse levels smooth with degree 2: their Galerkin rows are wide, and
     // one step less there costs fewer iterations than it saves
-    AMG_TRY(vcycle_coarse(c, d, 1, degree > AMG_COARSE_DEGREE ? AMG_COARSE_DEGREE : degree, &xc));
-    ka_prolong<<<grid_for(c, (const void*)ka_prolong, c->n), NT, 0, s>>>(c->n, L0.agg, xc,
-                                                                         d->scale, x0, c->d_st);
-    AMG_LAUNCH();
-    // level 0 post-smoothing; the last step forms z.r and beta
+    AMG_TRY(vcycle_coarse(c, d, 1, degree > AMG_COARSE_DEGREE ? AMG_COARSE_DEGREE : degree, B.Q,
+                          &xc));
+    // level 0 post-smoothing from x + a P x'; the last step forms z.r and beta
     float* xin = x0;
     float* xout = (x0 == Z[0]) ? Z[1] : Z[0];
-    ka_step<MW><<<grid_for(c, (const void*)ka_step<MW>, c->n), NT, 0, s>>>(
-        A, B.diag, B.rD, B.rA, xin, B.W1, xout, c->d_chebC, 0, c->d_st);
+    ka_step<MW, true><<<grid_for(c, (const void*)ka_step<MW, true>, c->n), NT, 0, s>>>(
+        A, B.diag, B.rD, B.rA, xin, L0.agg, xc, d->scale, B.W1, xout, c->d_chebC, 0, c->d_st);
     AMG_LAUNCH();
     std::swap(xin, xout);
     for (int j = 1; j < degree; ++j)
