@@ -12,7 +12,7 @@
 // level 0 is the context's matrix in its internal row order.  Each level's
 // cells are grouped into aggregates by root-based greedy aggregation along
 // the strong couplings of that solve's coefficients (a cell whose strong
-// neighbours are all free becomes a root and takes them; the others join
+// neighbours are all free becomes a root and takes up to 7 of them; the others join
 // the aggregate they are most strongly coupled to); the aggregates,
 // numbered in the order their roots are met, are the next level's cells.
 // Later solves keep the hierarchy and re-sum its operators.  The
@@ -25,15 +25,20 @@
 // (Gauss-Jordan, FP64) once per solve.
 //
 // V-cycle on level l (b = the level's right-hand side):
-//   x  = S(b)                  Chebyshev-Jacobi of degree nSweeps from 0
-//   r  = b - A x;  b' = P^T r;  x' = V-cycle(l+1, b');  x += P x'
+//   x  = S(b)                  Chebyshev-Jacobi from 0 (degree nSweeps on
+//                              level 0, 2 below)
+//   r  = b - A x;  b' = P^T r;  x' = V-cycle(l+1, b');  x += a P x'
 //   x += S(b - A x)            the same polynomial (symmetric cycle)
-// The smoother's interval is [beta/ratio, beta] with beta the Gershgorin
-// bound of D^-1 A on level 0 (metalFoamSolver.C:229-249) and ratio the
-// chebyshevRatio control; Galerkin levels of a diagonally dominant matrix
-// with non-positive off-diagonals keep that bound.  Level 0 reuses the
-// Krylov kernels (its pre-smoother start w0 = c1 rD r is formed by the
-// update kernel, its last post-smoothing step forms z.r and beta).
+// a = scaleCorrection, fixed in (0, 2), so the cycle is a fixed SPD
+// operator.  The smoother's interval is [beta/ratio, beta] with beta the
+// Gershgorin bound of D^-1 A on level 0 (metalFoamSolver.C:229-249) and
+// ratio the chebyshevRatio control; Galerkin levels of a diagonally
+// dominant matrix with non-positive off-diagonals keep that bound.  Level 0
+// reuses the Krylov kernels (its pre-smoother start w0 = c1 rD r is formed
+// by the update kernel, its last post-smoothing step forms z.r and beta).
+// The restriction is formed by the kernel that starts the next level, and
+// the prolongation by the first post-smoothing step, which reads x + a P x'
+// on the fly, so a coarse level costs five launches.
 #include "cudafoam.h"
 #include "cf_host.hpp"
 
