@@ -260,6 +260,9 @@ def time_cuda(fn, steps, stream):
     return e0.elapsed_time(e1)
 
 
+MANY_STREAMS = 8   # host threads / CUDA streams of the concurrent loop
+
+
 def run_batched(local, stream, ws=1, rank=0, steps=3):
     """48 independent pressure systems (log-uniform 1e3..1e6 cells): one
     batched solve vs the plain one-solve-at-a-time loop (graph-driven
@@ -347,6 +350,28 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
     ms_g = timed(plain(1, "GAMG"), steps) / steps
     it_g = [p.nIterations for p in res["p"]]
     ok_g = all(p.converged and p.finalResidual < 1e-6 for p in res["p"])
+
+    # the plain loop's solves run concurrently (cf_solve_many_device: host
+    # threads with their own streams); every system gets what its single
+    # solve returns
+    def many(precond):
+        oo = _lib.default_options(preconditioner=precond,
+                                  **(gamg_opts if precond == "GAMG" else opts))
+
+        def run():
+            for p in dp:
+                p.zero_()
+            if loc:
+                res["m"] = _lib.solve_many_device(ctxs, _lib.CF_SOLVER_PCG, dp, db, oo,
+                                                  streams=MANY_STREAMS, diags=dd, uppers=du)
+        return run
+
+    many_ms = {}
+    many_same = {}
+    for precond, its in (("Chebyshev", it_p), ("GAMG", it_g)):
+        many(precond)()
+        many_ms[precond] = timed(many(precond), steps) / steps
+        many_same[precond] = all(p.nIterations == q for p, q in zip(res.get("m", []), its))
     for c in ctxs:
         c.close()
     if bt is not None:
@@ -383,7 +408,19 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
                 "iterations_max": max(r["it"] for r in gam),
                 "iterations_total": sum(r["it"] for r in gam),
                 "chebyshev_iterations_total": sum(it_p) if ws == 1 else None,
-                "first_pass_ms_with_hierarchy_builds": round(setup_g, 1)}}
+                "first_pass_ms_with_hierarchy_builds": round(setup_g, 1)},
+            "concurrent_streams": {
+                "note": f"the plain loop on {MANY_STREAMS} host threads with their own CUDA "
+                        "streams (cf_solve_many_device), one context per system, largest "
+                        "systems first; each system's result equals its single solve",
+                "chebyshev_ms": round(many_ms["Chebyshev"], 2),
+                "chebyshev_solves_per_s": round(S / (many_ms["Chebyshev"] / 1e3), 2),
+                "chebyshev_speedup_vs_plain_loop": round(ms_p / many_ms["Chebyshev"], 3),
+                "chebyshev_speedup_vs_batched": round(ms_b / many_ms["Chebyshev"], 3),
+                "gamg_ms": round(many_ms["GAMG"], 2),
+                "gamg_solves_per_s": round(S / (many_ms["GAMG"] / 1e3), 2),
+                "gamg_speedup_vs_batched_chebyshev": round(ms_b / many_ms["GAMG"], 3),
+                "iterations_identical_to_single": bool(all(many_same.values()))}}
 
 
 def run_adjoint(local, stream, steps=3):

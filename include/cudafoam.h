@@ -438,6 +438,22 @@ int cf_set_spmv_config(cf_context* ctx, const cf_spmv_config* cfg);
 int cf_autotune(cf_context* ctx, int32_t reps, int32_t apply, cf_spmv_config* best,
                 cf_tune_entry* table, int32_t capacity, int32_t* count);
 
+/* ------------------------------------------------------------ many systems */
+/* Independent systems, one context each (topology set), solved concurrently:
+ * `streams` host threads (1..64), each with its own CUDA stream, take the
+ * systems largest first and, for each, stage the coefficients when diag is
+ * not NULL (cf_set_coeffs_device with diag[i], upper[i], lower ? lower[i] :
+ * NULL) and run cf_solve_device(ctx[i], solver, psi[i], source[i], opts,
+ * &perf[i]).  All pointers are device pointers; work queued earlier on any
+ * stream completes first, and everything is complete on return.  Every
+ * system gets exactly what cf_solve_device on it alone returns.  A context
+ * may appear once.  No counterpart in the reference. */
+int cf_solve_many_device(cf_context* const* ctx, int32_t count, int32_t solver,
+                         double* const* psi, const double* const* source,
+                         const double* const* diag, const double* const* upper,
+                         const double* const* lower, const cf_options* opts, int32_t streams,
+                         cf_performance* perf);
+
 /* ------------------------------------------------------------ GAMG */
 /* Cells of every level of the context's multigrid hierarchy (built by the
  * first cudaPCG solve with CF_PRECOND_GAMG on the current topology; level 0

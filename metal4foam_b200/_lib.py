@@ -129,6 +129,9 @@ SIGNATURES = [
     ("cf_autotune", C.c_int, [vp, i32, i32, C.POINTER(SpmvConfig), C.POINTER(TuneEntry), i32,
                               C.POINTER(i32)]),
     ("cf_gamg_levels", C.c_int, [vp, C.POINTER(i32), i32, C.POINTER(i32)]),
+    ("cf_solve_many_device", C.c_int, [C.POINTER(vp), i32, i32, C.POINTER(vp), C.POINTER(vp),
+                                       C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                       C.POINTER(Options), i32, vp]),
     ("cf_gamg_export", C.c_int, [vp, i32, C.POINTER(i32), vp, vp, vp, vp, vp]),
     ("cf_solve_multi", C.c_int, [vp, i32, i32, vp, vp, C.POINTER(Options),
                                  C.POINTER(Performance)]),
@@ -203,6 +206,26 @@ def ptr(a):
             raise ValueError("tensor must be contiguous")
         return vp(a.data_ptr())
     raise TypeError(f"unsupported array type {type(a)}")
+
+
+def solve_many_device(contexts, solver, psis, sources, options, streams=8, diags=None,
+                      uppers=None, lowers=None):
+    """cf_solve_many_device: independent systems (one Context each) solved
+    concurrently on `streams` host threads / CUDA streams; device arrays
+    (torch tensors); coefficients staged first when diags is given.
+    Returns one Performance per system."""
+    n = len(contexts)
+    arr = vp * max(n, 1)
+    ctx = arr(*[c.h for c in contexts])
+    ps = arr(*[ptr(x) for x in psis])
+    ss = arr(*[ptr(x) for x in sources])
+    ds = arr(*[ptr(x) for x in diags]) if diags is not None else None
+    us = arr(*[ptr(x) for x in uppers]) if uppers is not None else None
+    ls = arr(*[ptr(x) for x in lowers]) if lowers is not None else None
+    perf = (Performance * max(n, 1))()
+    check(load().cf_solve_many_device(ctx, int(n), int(solver), ps, ss, ds, us, ls,
+                                      C.byref(options), int(streams), perf))
+    return list(perf)[:n]
 
 
 def default_options(**kw):
