@@ -82,9 +82,21 @@ extern "C" int cf_solve_many_device(cf_context* const* ctx, int32_t count, int32
         }
     };
     std::vector<std::thread> pool;
+    std::vector<int> inline_shares;   // shares whose thread could not be started
     pool.reserve(W);
-    for (int w = 1; w < W; ++w) pool.emplace_back(worker, w);
+    for (int w = 1; w < W; ++w)
+    {
+        try
+        {
+            pool.emplace_back(worker, w);
+        }
+        catch (...)
+        {
+            inline_shares.push_back(w);   // no exception crosses the C ABI
+        }
+    }
     worker(0);
+    for (int w : inline_shares) worker(w);
     for (auto& t : pool) t.join();
     for (int w = 0; w < W; ++w)
     {
