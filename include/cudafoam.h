@@ -124,7 +124,9 @@ typedef struct
                                   solve, Chebyshev-Jacobi smoothing on
                                   [beta/chebyshevRatio, beta], the coarsest
                                   level inverted densely); the FP64 driver
-                                  is unchanged.  Default SpMV shape only.  */
+                                  is unchanged.  The V-cycle runs its own
+                                  SELL-32 kernels whatever the SpMV launch
+                                  shape (cf_set_spmv_config) is.           */
     int32_t nSweeps;           /* GAMG: Chebyshev degree of the smoother,
                                   2..8, default 3                          */
     int32_t nCellsInCoarsestLevel; /* GAMG: coarsening stops at this many

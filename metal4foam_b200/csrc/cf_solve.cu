@@ -365,8 +365,6 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
     const bool gamg = o->preconditioner == CF_PRECOND_GAMG;
     if (gamg && bicg)
         return fail(CF_ERR_UNSUPPORTED, "the GAMG preconditioner is offered for cudaPCG only");
-    if (gamg && !spmv_default(c))
-        return fail(CF_ERR_UNSUPPORTED, "the GAMG preconditioner runs in the default SpMV shape");
     // the V-cycle replaces the Chebyshev apply for this solve only
     struct AmgScope
     {
