@@ -1444,6 +1444,9 @@ static int batch_check(cf_batch* bt, int32_t solver, const cf_options* o, cf_per
     if (solver != CF_SOLVER_PCG)
         return fail(CF_ERR_UNSUPPORTED, "batched solves are cudaPCG (symmetric pressure systems)");
     if (!o || !perf || !psi || !src) return fail(CF_ERR_INVALID_ARG, "NULL argument");
+    if (o->preconditioner != CF_PRECOND_CHEBYSHEV)
+        return fail(CF_ERR_UNSUPPORTED, "batched solves use the Chebyshev-Jacobi preconditioner "
+                                        "(GAMG systems: one context each, cf_solve_many_device)");
     if (o->chebyshevOrder < 1 || o->chebyshevOrder > CF_MAX_CHEB)
         return fail(CF_ERR_INVALID_ARG, "chebyshevOrder must be in [1, 64]");
     if (o->deflate < CF_DEFLATE_AUTO || o->deflate > CF_DEFLATE_OFF)

@@ -993,6 +993,9 @@ int solve_multi(cf_context* c, int32_t solver, int32_t nrhs, double* psi, const 
     if (!psi || !src || !o || !perf) return fail(CF_ERR_INVALID_ARG, "NULL argument");
     if (solver != CF_SOLVER_PBICGSTAB)
         return fail(CF_ERR_UNSUPPORTED, "multi-RHS solves are cudaPBiCGStab (momentum)");
+    if (o->preconditioner != CF_PRECOND_CHEBYSHEV)
+        return fail(CF_ERR_UNSUPPORTED, "multi-RHS solves use the Jacobi preconditioner of "
+                                        "cudaPBiCGStab (GAMG preconditions cudaPCG)");
     if (nrhs < 1) return fail(CF_ERR_INVALID_ARG, "nrhs must be >= 1");
     CF_CUDA(cudaSetDevice(c->device));
     if (c->transposed) return fail(CF_ERR_UNSUPPORTED, "transposed operator staged");

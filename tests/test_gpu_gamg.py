@@ -144,7 +144,22 @@ def test_gamg_rejects(require_gpu):
             ctx.solve(PCG, np.zeros(s.n), s.source, _lib.default_options(**kw))
         assert ei.value.code == 1, bad
     assert ctx.gamg_levels() == []
+    # the multi-RHS (BiCGStab) and batched paths do not offer it
+    with pytest.raises(_lib.CudaFoamError) as ei:
+        ctx.solve_multi(_lib.CF_SOLVER_PBICGSTAB, np.zeros((2, s.n)),
+                        np.ascontiguousarray(np.stack([s.source, s.source])),
+                        _lib.default_options(preconditioner="GAMG"))
+    assert ei.value.code == 8
     ctx.close()
+    sym = mesh.varcoeff3d((8, 7, 6), seed=18, permute=False)
+    bt = _lib.Batch(0)
+    bt.add_system(sym.addr)
+    bt.finalize()
+    bt.set_coeffs(0, sym.diag, sym.upper)
+    with pytest.raises(_lib.CudaFoamError) as ei:
+        bt.solve([np.zeros(sym.n)], [sym.source], _lib.default_options(preconditioner="GAMG"))
+    assert ei.value.code == 8
+    bt.close()
 
 
 def test_gamg_whatever_the_spmv_shape(require_gpu):
