@@ -4,8 +4,10 @@
  * losort, losortStart), fixes cell 0 (diag doubled, as OpenFOAM's
  * setReference), and solves it with cf_solve (cudaPCG) to 1e-6.
  *
- *   solve_poisson nx ny nz
+ *   solve_poisson nx ny nz [GAMG]
  *
+ * With GAMG the inner PCG is preconditioned by the multigrid V-cycle
+ * (cf_options.preconditioner = CF_PRECOND_GAMG) instead of Chebyshev-Jacobi.
  * Prints "status <code>" and, on success, the solverPerformance figures and
  * the FP64 residual recomputed here from psi.  Exits 0 on CF_OK, 3 when no
  * sm_100 device is present (CF_ERR_NO_DEVICE), 1 otherwise.
@@ -13,6 +15,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include "cudafoam.h"
 
@@ -65,6 +68,7 @@ int main(int argc, char** argv)
     if (rc == CF_OK) rc = cf_set_coeffs(ctx, diag, upper, NULL, NULL);
     cf_options o;
     cf_options_default(&o);
+    if (argc > 4 && strcmp(argv[4], "GAMG") == 0) o.preconditioner = CF_PRECOND_GAMG;
     cf_performance perf;
     if (rc == CF_OK) rc = cf_solve(ctx, CF_SOLVER_PCG, psi, src, &o, &perf);
     printf("status %d %s\n", rc, rc == CF_OK ? "" : cf_last_error());

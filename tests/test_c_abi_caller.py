@@ -36,8 +36,9 @@ def test_c_caller_without_device(tmp_path):
 
 
 @pytest.mark.gpu
-def test_c_caller_solves(require_gpu, tmp_path):
-    res = run(build_caller(tmp_path), 24, 20, 16)
+@pytest.mark.parametrize("precond", ["Chebyshev", "GAMG"])
+def test_c_caller_solves(require_gpu, tmp_path, precond):
+    res = run(build_caller(tmp_path), 24, 20, 16, precond)
     assert res.returncode == 0, res.stdout + res.stderr
     line = res.stdout.strip().splitlines()[-1].split()
     vals = dict(zip(line[0::2], line[1::2]))
