@@ -43,6 +43,7 @@
 #include "cf_host.hpp"
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -668,7 +669,7 @@ int amg_level_cells(const cf_context* c, int l)
 }
 
 // Hierarchy of the context's topology (host aggregation, device layouts).
-int amg_prepare(cf_context* c, int coarsestCap)
+int amg_prepare(cf_context* c, int coarsestCap, bool profile)
 {
     AmgData* old = static_cast<AmgData*>(c->amg);
     if (old && old->coarsestCap == coarsestCap) return CF_OK;
@@ -676,6 +677,8 @@ int amg_prepare(cf_context* c, int coarsestCap)
     AmgData* d = new AmgData();
     c->amg = d;
     d->coarsestCap = coarsestCap;
+    const double t0 = wall_now();
+    double tAgg = 0.0, tCoarse = 0.0, tLayout = 0.0;
     const int n = c->n;
     const int nf = c->nf;
     // level-0 faces in the internal row order (the caller's face order kept,
@@ -718,6 +721,7 @@ int amg_prepare(cf_context* c, int coarsestCap)
     {
         const int nl = d->lv[cur].n;
         const int nfl = (int)lo.size();
+        const double ta = wall_now();
         std::vector<int> xadj, adj, adjFace, agg;
         csr_of_faces(nl, lo, up, xadj, adj, adjFace);
         std::vector<double> str(adj.size());
@@ -728,6 +732,8 @@ int amg_prepare(cf_context* c, int coarsestCap)
                 str[q] = dd > 0.0 ? std::fabs(hu[adjFace[q]]) / std::sqrt(dd) : 0.0;
             }
         const int nagg = aggregate(nl, xadj, adj, str, agg);
+        const double tb = wall_now();
+        tAgg += tb - ta;
         if (nagg >= nl || nagg < 1) break;   // no coarsening possible
         // members of each aggregate (ascending rows)
         std::vector<int> aggStart(nagg + 1, 0), aggRows(nl);
@@ -739,8 +745,10 @@ int amg_prepare(cf_context* c, int coarsestCap)
         }
         // faces inside aggregates, and coarse faces (owner < neighbour, sorted)
         std::vector<int> intStart(nagg + 1, 0), intList;
-        std::vector<std::pair<uint64_t, int>> between;
-        between.reserve(nfl);
+        // faces between aggregates, grouped by their lower aggregate
+        // (counting sort), then each group ordered by (upper aggregate,
+        // face): the order of a full sort by (pair, face), in linear time
+        std::vector<int> bstart(nagg + 1, 0);
         for (int f = 0; f < nfl; ++f)
         {
             const int a = agg[lo[f]];
@@ -748,8 +756,21 @@ int amg_prepare(cf_context* c, int coarsestCap)
             if (a == b)
                 ++intStart[a + 1];
             else
-                between.push_back({((uint64_t)std::min(a, b) << 32) | (uint64_t)std::max(a, b), f});
+                ++bstart[std::min(a, b) + 1];
         }
+        for (int k = 0; k < nagg; ++k) bstart[k + 1] += bstart[k];
+        std::vector<std::pair<int, int>> between(bstart[nagg]);   // (upper aggregate, face)
+        {
+            std::vector<int> pos(bstart.begin(), bstart.end() - 1);
+            for (int f = 0; f < nfl; ++f)
+            {
+                const int a = agg[lo[f]];
+                const int b = agg[up[f]];
+                if (a != b) between[pos[std::min(a, b)]++] = {std::max(a, b), f};
+            }
+        }
+        for (int k = 0; k < nagg; ++k)
+            std::sort(between.begin() + bstart[k], between.begin() + bstart[k + 1]);
         for (int k = 0; k < nagg; ++k) intStart[k + 1] += intStart[k];
         intList.assign(intStart[nagg], 0);
         {
@@ -760,20 +781,22 @@ int amg_prepare(cf_context* c, int coarsestCap)
                 if (a == agg[up[f]]) intList[pos[a]++] = f;
             }
         }
-        std::sort(between.begin(), between.end());
         std::vector<int> clo, cup, cfStart, cfList(between.size());
-        for (size_t q = 0; q < between.size(); ++q)
-        {
-            if (q == 0 || between[q].first != between[q - 1].first)
+        for (int k = 0; k < nagg; ++k)
+            for (int q = bstart[k]; q < bstart[k + 1]; ++q)
             {
-                cfStart.push_back((int)q);
-                clo.push_back((int)(between[q].first >> 32));
-                cup.push_back((int)(between[q].first & 0xffffffffu));
+                if (q == bstart[k] || between[q].first != between[q - 1].first)
+                {
+                    cfStart.push_back(q);
+                    clo.push_back(k);
+                    cup.push_back(between[q].first);
+                }
+                cfList[q] = between[q].second;
             }
-            cfList[q] = between[q].second;
-        }
         cfStart.push_back((int)between.size());
         const int nfc = (int)clo.size();
+        const double tc = wall_now();
+        tCoarse += tc - tb;
 
         AmgLevel& L = d->lv[cur];
         L.nagg = nagg;
@@ -803,8 +826,10 @@ int amg_prepare(cf_context* c, int coarsestCap)
             for (int F = 0; F < nfc; ++F) los[pos[cup[F]]++] = F;
         }
         HostLayout H;
+        const double tl = wall_now();
         AMG_TRY(build_layout(nagg, nfc, clo.data(), cup.data(), own.data(), los.data(),
                              losS.data(), false, H));
+        tLayout += wall_now() - tl;
         d->lv.emplace_back();
         AmgLevel& C = d->lv.back();
         C.n = nagg;
@@ -866,6 +891,16 @@ int amg_prepare(cf_context* c, int coarsestCap)
     AMG_TRY(amg_alloc(c, d, &d->scale, 1));
     AMG_TRY(amg_alloc(c, d, &d->coarseInv, (size_t)Z.n * Z.n));
     AMG_CUDA(cudaStreamSynchronize(c->stream));
+    if (profile)
+    {
+        std::printf("    GAMG hierarchy: %d levels (", (int)d->lv.size());
+        for (size_t l = 0; l < d->lv.size(); ++l)
+            std::printf("%s%d", l ? " / " : "", d->lv[l].n);
+        std::printf(" cells) built in %.1f ms: aggregation %.1f, coarse faces %.1f, "
+                    "layouts %.1f, rest (copies, uploads) %.1f\n",
+                    1e3 * (wall_now() - t0), 1e3 * tAgg, 1e3 * tCoarse, 1e3 * tLayout,
+                    1e3 * (wall_now() - t0 - tAgg - tCoarse - tLayout));
+    }
     return CF_OK;
 }
 

@@ -200,7 +200,7 @@ int persistent_status(cf_context* c);
 // hierarchy of the topology down to at most coarsestCap (<= 128) cells,
 // coefficients of every level from the staged operator (deflated or not),
 // and one inner iteration with the V-cycle as z = M r.
-int amg_prepare(cf_context* c, int coarsestCap);
+int amg_prepare(cf_context* c, int coarsestCap, bool profile = false);
 int amg_stage(cf_context* c, int deflate, float scaleCorrection);
 int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int useCond,
                     int* kernels);

@@ -421,7 +421,7 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
         CF_TRY(stage_diag32(c, deflate ? 1 : 0));
         if (gamg)
         {
-            CF_TRY(amg_prepare(c, o->nCellsInCoarsestLevel));
+            CF_TRY(amg_prepare(c, o->nCellsInCoarsestLevel, o->profile != 0));
             CF_TRY(amg_stage(c, deflate ? 1 : 0, (float)o->scaleCorrection));
             c->amgActive = true;
         }

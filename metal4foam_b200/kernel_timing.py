@@ -88,7 +88,7 @@ def gamg(dims):
     a = s.addr
     ctx.set_topology(a.n, a.nf, *a.arrays())
     ctx.set_coeffs(s.diag, s.upper, None)
-    opts = _lib.default_options(preconditioner="GAMG", graph=0)
+    opts = _lib.default_options(preconditioner="GAMG", graph=0, profile=True)
     for k in range(2):
         psi = np.zeros(s.n)
         t0 = time.perf_counter()
