@@ -63,9 +63,12 @@ def test_transpose_operator(require_gpu, oracle):
     ctx.close()
 
 
-@pytest.mark.parametrize("kind", ["symmetric", "asymmetric"])
+@pytest.mark.parametrize("kind", ["symmetric", "asymmetric", "symmetric_gamg"])
 def test_adjoint_vs_fp64_cpu_adjoint(require_gpu, oracle, kind):
-    if kind == "symmetric":
+    """symmetric_gamg: forward and adjoint solves preconditioned by the
+    opt-in multigrid V-cycle, checked against the same FP64 reference."""
+    extra = dict(preconditioner="GAMG") if kind == "symmetric_gamg" else {}
+    if kind.startswith("symmetric"):
         s, xstar = mesh.adjoint_system((20, 20, 20), seed=43)
         solver = _lib.CF_SOLVER_PCG
     else:
@@ -77,12 +80,12 @@ def test_adjoint_vs_fp64_cpu_adjoint(require_gpu, oracle, kind):
     a = s.addr
     ctx.set_topology(a.n, a.nf, *a.arrays())
     ctx.set_coeffs(s.diag, s.upper, s.lower)
-    opts = _lib.default_options(**TIGHT)
+    opts = _lib.default_options(**TIGHT, **extra)
     x = np.zeros(s.n)
     p = ctx.solve(solver, x, s.source, opts)
     assert p.converged and p.finalResidual < 1e-10
     lam, dU, dL, dD, pa = ctx.solve_adjoint(solver, x, x - xstar, s.nf,
-                                            _lib.default_options(**ADJ))
+                                            _lib.default_options(**ADJ, **extra))
     assert pa.converged and pa.finalResidual < 1e-9
     assert rel_err(x, x_ref) < 1e-6
     assert rel_err(lam, lam_ref) < 1e-4
