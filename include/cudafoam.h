@@ -122,7 +122,7 @@ typedef struct
                                   V-cycle over aggregation levels (Galerkin
                                   coarse operators summed on the device each
                                   solve, Chebyshev-Jacobi smoothing on
-                                  [beta/chebyshevRatio, beta], the coarsest
+                                  [beta/smootherRatio, beta], the coarsest
                                   level inverted densely); the FP64 driver
                                   is unchanged.  The V-cycle runs its own
                                   SELL-32 kernels whatever the SpMV launch
@@ -135,6 +135,10 @@ typedef struct
                                   correction, in (0, 2) (the cycle stays
                                   symmetric positive definite), default
                                   1.8 (plain aggregation under-corrects)   */
+    double smootherRatio;      /* GAMG: the smoother's Chebyshev interval is
+                                  [beta/smootherRatio, beta] (> 1, default
+                                  8); chebyshevRatio keeps its meaning for
+                                  the Chebyshev-Jacobi preconditioner     */
 } cf_options;
 
 /* solverPerformance plus the reference's profile/verbose figures
@@ -169,7 +173,7 @@ const char* cf_last_error(void);
 /* fills defaults: tolerance 1e-6, relTol 0, maxIter 1000, minIter 0,
  * maxRestarts 8, iterationsPerSync 1, deflate auto, chebyshevOrder 8,
  * chebyshevRatio 30, graph 1, preconditioner Chebyshev, nSweeps 3,
- * nCellsInCoarsestLevel 128, scaleCorrection 1.8 */
+ * nCellsInCoarsestLevel 128, scaleCorrection 1.8, smootherRatio 8 */
 void cf_options_default(cf_options* opts);
 
 /* ------------------------------------------------------------ context */

@@ -53,6 +53,7 @@ class Options(C.Structure):
         ("clusterMaxCells", C.c_int32),
         ("preconditioner", C.c_int32), ("nSweeps", C.c_int32),
         ("nCellsInCoarsestLevel", C.c_int32), ("scaleCorrection", C.c_double),
+        ("smootherRatio", C.c_double),
     ]
 
 

@@ -411,6 +411,7 @@ extern "C" void cf_options_default(cf_options* o)
     o->nSweeps = 3;
     o->nCellsInCoarsestLevel = 128;
     o->scaleCorrection = 1.8;
+    o->smootherRatio = 8.0;
 }
 
 extern "C" int cf_context_create(cf_context** out, int32_t device)

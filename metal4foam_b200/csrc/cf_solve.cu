@@ -436,7 +436,7 @@ int solve_device(cf_context* c, int solver, double* psi_dev, const double* src_d
             auto fn = k_gershgorin<MW>;
             fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(
                 A, c->d_eface, c->d_upper, c->d_diag64, c->d_u, deflate ? 1 : 0, order,
-                o->chebyshevRatio, c->d_chebC, c->d_drv, c->d_part);
+                gamg ? o->smootherRatio : o->chebyshevRatio, c->d_chebC, c->d_drv, c->d_part);
             CF_LAUNCH();
         }
         CF_TRY(fetch_drv(c));
@@ -560,10 +560,10 @@ int check_options(const cf_options* o)
     if (o->preconditioner == CF_PRECOND_GAMG &&
         (o->nSweeps < 2 || o->nSweeps > 8 || o->nCellsInCoarsestLevel < 1 ||
          o->nCellsInCoarsestLevel > 128 || !(o->scaleCorrection > 0.0) ||
-         !(o->scaleCorrection < 2.0)))
+         !(o->scaleCorrection < 2.0) || !(o->smootherRatio > 1.0)))
         return fail(CF_ERR_INVALID_ARG, "GAMG: nSweeps must be in [2, 8], "
-                                        "nCellsInCoarsestLevel in [1, 128] and "
-                                        "scaleCorrection in (0, 2)");
+                                        "nCellsInCoarsestLevel in [1, 128], "
+                                        "scaleCorrection in (0, 2) and smootherRatio > 1");
     return CF_OK;
 }
 

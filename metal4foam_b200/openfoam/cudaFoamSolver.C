@@ -215,6 +215,7 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     opts.nSweeps = cudaDict_.getOrDefault<label>("nSweeps", 3);
     opts.nCellsInCoarsestLevel = cudaDict_.getOrDefault<label>("nCellsInCoarsestLevel", 128);
     opts.scaleCorrection = cudaDict_.getOrDefault<scalar>("scaleCorrection", 1.8);
+    opts.smootherRatio = cudaDict_.getOrDefault<scalar>("smootherRatio", 8.0);
 
     // autotune yes: time the SpMV launch shapes once per context (the mesh
     // of a context does not change during a run) and keep the fastest

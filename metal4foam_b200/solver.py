@@ -145,7 +145,7 @@ def backend_cache_clear():
 _CONTROL_KEYS = ("maxRestarts", "iterationsPerSync", "deflate", "chebyshevOrder",
                  "chebyshevRatio", "profile", "verbose", "graph", "stagnationLimit", "autotune",
                  "persistentMaxCells", "clusterMaxCells", "preconditioner", "nSweeps",
-                 "nCellsInCoarsestLevel", "scaleCorrection")
+                 "nCellsInCoarsestLevel", "scaleCorrection", "smootherRatio")
 
 def _preconditioner(name) -> int:
     """`preconditioner` of the cuda sub-dictionary: Chebyshev (the
@@ -175,8 +175,8 @@ class cudaFoamSolver:
     :mod:`metal4foam_b200.autotune`), ``persistentMaxCells``,
     ``clusterMaxCells`` and, for cudaPCG, ``preconditioner`` (Chebyshev,
     the reference's default, or GAMG: one aggregation multigrid V-cycle per
-    inner iteration) with ``nSweeps``, ``nCellsInCoarsestLevel`` and
-    ``scaleCorrection``.
+    inner iteration) with ``nSweeps``, ``nCellsInCoarsestLevel``,
+    ``scaleCorrection`` and ``smootherRatio``.
     """
 
     typeName = "cudaFoamSolver"
@@ -229,6 +229,7 @@ class cudaFoamSolver:
             nSweeps=int(s.get("nSweeps", 3)),
             nCellsInCoarsestLevel=int(s.get("nCellsInCoarsestLevel", 128)),
             scaleCorrection=float(s.get("scaleCorrection", 1.8)),
+            smootherRatio=float(s.get("smootherRatio", 8.0)),
         )
 
     def solveImpl(self, psi: np.ndarray, source: np.ndarray, cmpt: int = 0) -> solverPerformance:

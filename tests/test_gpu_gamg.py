@@ -137,7 +137,8 @@ def test_gamg_rejects(require_gpu):
     assert ei.value.code == 8
     for bad in (dict(nSweeps=1), dict(nSweeps=9), dict(nCellsInCoarsestLevel=0),
                 dict(nCellsInCoarsestLevel=129), dict(preconditioner=7),
-                dict(scaleCorrection=0.0), dict(scaleCorrection=2.0)):
+                dict(scaleCorrection=0.0), dict(scaleCorrection=2.0),
+                dict(smootherRatio=1.0)):
         kw = dict(preconditioner="GAMG")
         kw.update(bad)
         with pytest.raises(_lib.CudaFoamError) as ei:
