@@ -32,7 +32,7 @@
 // a = scaleCorrection, fixed in (0, 2), so the cycle is a fixed SPD
 // operator.  The smoother's interval is [beta/ratio, beta] with beta the
 // Gershgorin bound of D^-1 A on level 0 (metalFoamSolver.C:229-249) and
-// ratio the chebyshevRatio control; Galerkin levels of a diagonally
+// ratio the smootherRatio control (default 8); Galerkin levels of a diagonally
 // dominant matrix with non-positive off-diagonals keep that bound.  Level 0
 // reuses the Krylov kernels (its pre-smoother start w0 = c1 rD r is formed
 // by the update kernel, its last post-smoothing step forms z.r and beta).
