@@ -193,6 +193,12 @@ int cf_context_set_stream(cf_context* ctx, void* stream);
  * for meshes above 65536 cells).  Results are returned in the caller's
  * ordering either way. */
 int cf_context_set_reorder(cf_context* ctx, int32_t mode);
+/* Polls a bounded device-side wait of this context (the grid barriers of
+ * persistent inner solves, persistentMaxCells) makes before it gives up;
+ * a wait that gives up ends the kernel and the solve returns
+ * CF_ERR_DEVICE_TIMEOUT, leaving the context usable.  0 restores the
+ * default, 2^24 polls of about 64 ns each.  No reference counterpart. */
+int cf_context_set_wait_limit(cf_context* ctx, int64_t polls);
 /* Number of kernels this context has launched so far (graph bodies are
  * counted once per executed iteration).  Diagnostic; no reference
  * counterpart. */
@@ -387,6 +393,80 @@ enum
 int cf_time_kernel(cf_context* ctx, int32_t which, int32_t reps,
                    double* msPerLaunch);
 
+/* ------------------------------------------------------------ kernel check */
+/* One launch of a fused inner-iteration kernel on caller-supplied vectors
+ * and scalars, exactly as the inner loop launches it (same kernel, launch
+ * shape and buffers; iteration 0 of a live solve), for comparison with the
+ * reference's unfused kernel sequence (metalFoamKernels.metal:64-276,
+ * 372-458).  Diagnostic; no reference counterpart.  Host pointers, nCells
+ * floats each, caller's cell order; the FP32 matrix, diag and rD are those
+ * staged by the last cf_set_coeffs / solve.  alpha, beta, omega are the
+ * solver scalars (the kernel rounds them to FP32 as the loop does).  sums
+ * receives the step's reductions (products of FP32 values accumulated in
+ * FP64).  The context's work vectors are overwritten.
+ *
+ *   CF_STEP_CHEB        in zIn, wIn, rA; chebOrder, chebStep (1..order-1),
+ *                       chebBeta, chebRatio -> v = A zIn,
+ *                       wOut = c2 wIn + c3 rD (rA - v), zOut = zIn + wOut;
+ *                       sums[0] = zOut.rA on the last step
+ *   CF_STEP_PCG_P_SPMV  in wA, pOld; beta -> p = wA + beta pOld, q = A p;
+ *                       sums[0] = p.q
+ *   CF_STEP_PCG_UPDATE  in delta, p, rA, q; alpha; chebOrder (1: Jacobi)
+ *                       -> deltaNext = delta + alpha p, rAOut = rA - alpha q,
+ *                       wAOut = c1 rD rAOut (Chebyshev start) or
+ *                       rAOut rD (Jacobi); sums[0] = sum|rAOut|,
+ *                       sums[1] = wAOut.rAOut (Jacobi)
+ *   CF_STEP_BICG_AB     in rA, pOld, AyAOld, rA0; beta, omega
+ *                       -> p = rA + beta (pOld - omega AyAOld), yA = rD p,
+ *                       AyA = A yA; sums[0] = rA0.AyA
+ *   CF_STEP_BICG_CD     in rA, AyA; alpha -> sA = rA - alpha AyA,
+ *                       zA = rD sA, tA = A zA; sums = sum|sA|, sA.tA, tA.tA
+ *   CF_STEP_BICG_E      in delta, yA, zA, sA, tA, rA0; alpha, omega
+ *                       -> deltaNext = delta + (alpha yA + omega zA),
+ *                       rAOut = sA - omega tA; sums = sum|rAOut|, rA0.rAOut
+ */
+enum
+{
+    CF_STEP_CHEB = 0,
+    CF_STEP_PCG_P_SPMV = 1,
+    CF_STEP_PCG_UPDATE = 2,
+    CF_STEP_BICG_AB = 3,
+    CF_STEP_BICG_CD = 4,
+    CF_STEP_BICG_E = 5
+};
+
+typedef struct cf_step_io
+{
+    const float* rA;
+    const float* rA0;
+    const float* wA;
+    const float* pOld;
+    const float* AyAOld;
+    const float* delta;
+    const float* zIn;
+    const float* wIn;
+    float* p;             /* in for PCG_UPDATE, out for P_SPMV and BICG_AB   */
+    float* q;             /* in for PCG_UPDATE, out for P_SPMV               */
+    float* yA;            /* in for BICG_E, out for BICG_AB                  */
+    float* AyA;           /* in for BICG_CD, out for BICG_AB                 */
+    float* sA;            /* in for BICG_E, out for BICG_CD                  */
+    float* zA;            /* in for BICG_E, out for BICG_CD                  */
+    float* tA;            /* in for BICG_E, out for BICG_CD                  */
+    float* deltaNext;
+    float* rAOut;
+    float* wAOut;
+    float* wOut;
+    float* zOut;
+    double alpha, beta, omega;
+    int32_t chebOrder;
+    int32_t chebStep;
+    double chebBeta;
+    double chebRatio;
+    double sums[3];
+} cf_step_io;
+
+int cf_inner_step(cf_context* ctx, int32_t step, cf_step_io* io);
+
 /* ------------------------------------------------------------ autotuning */
 /* No counterpart in the reference (the design's autotuner row).  The SpMV
  * inside the FP32 Krylov kernels (Chebyshev steps, p-update SpMV, both
@@ -450,8 +530,10 @@ int cf_autotune(cf_context* ctx, int32_t reps, int32_t apply, cf_spmv_config* be
  * systems largest first and, for each, stage the coefficients when diag is
  * not NULL (cf_set_coeffs_device with diag[i], upper[i], lower ? lower[i] :
  * NULL) and run cf_solve_device(ctx[i], solver, psi[i], source[i], opts,
- * &perf[i]).  All pointers are device pointers; work queued earlier on any
- * stream completes first, and everything is complete on return.  Every
+ * &perf[i]).  All contexts must be on one device (CF_ERR_INVALID_ARG
+ * otherwise); all pointers are device pointers on it; work queued earlier on
+ * any stream of that device completes first, and everything is complete on
+ * return.  Every
  * system gets exactly what cf_solve_device on it alone returns.  A context
  * may appear once.  No counterpart in the reference. */
 int cf_solve_many_device(cf_context* const* ctx, int32_t count, int32_t solver,
@@ -483,20 +565,24 @@ int cf_gamg_export(cf_context* ctx, int32_t level, int32_t* nFaces, int32_t* agg
  * their own pre-allocated buffers.  No counterpart in the reference.
  *
  * Everything is a device pointer on the current device and is owned by the
- * caller: the LDU arrays as cf_set_topology takes them, FP32 coefficients
- * (lower NULL: symmetric), x, w (NULL: dot = 0), y and dot (one double;
- * NULL: no dot).  The row sums use the reference kernel's order (diagonal,
- * owner-side faces, then losort faces).  The call is asynchronous on
- * `stream` (a cudaStream_t, NULL: the default stream) and calls no
- * cudaMalloc, cudaFree or allocating library routine: the per-block
- * partial sums live in a fixed file-scope device array of 65,536 doubles
- * plus one 256-byte line, which every GPU that loads the library keeps until
- * the process exits.  Hence nCells is limited to 16,777,216; larger sizes
- * return CF_ERR_TOO_LARGE before anything is launched.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress): make
- * it before any stream capture.  All calls on a device share the array, so
- * calls whose kernels overlap on the GPU (different streams without
- * ordering) race and give wrong dot products. */
+ * caller: the LDU arrays as cf_set_topology takes them (none may be NULL;
+ * a mesh without faces passes any valid device pointer for the face
+ * arrays), FP32 coefficients (lower NULL: symmetric), x, w (NULL: dot = 0),
+ * y and dot (one double; NULL: no dot).  NULL where a pointer is required
+ * returns CF_ERR_INVALID_ARG before anything is launched.  The row sums use
+ * the reference kernel's order (diagonal, owner-side faces, then losort
+ * faces).  The call is asynchronous on `stream` (a cudaStream_t, NULL: the
+ * default stream) and calls no cudaMalloc, cudaFree or allocating library
+ * routine: the per-block partial sums live in a fixed file-scope device
+ * array of 65,536 doubles plus one 256-byte line, which every GPU that loads
+ * the library keeps until the process exits.  Hence nCells is limited to
+ * 16,777,216; larger sizes return CF_ERR_TOO_LARGE before anything is
+ * launched.  The first call in a CUDA context looks up that array's device
+ * address (cudaGetSymbolAddress) and caches it for the context: make it
+ * before any stream capture (made while `stream` is capturing, it returns
+ * CF_ERR_UNSUPPORTED and launches nothing).  All calls on a device share the
+ * array, so calls whose kernels overlap on the GPU (different streams
+ * without ordering) race and give wrong dot products. */
 int cf_ldu_spmv_dot_noalloc(int32_t nCells, const float* diag,
                             const float* upper, const float* lower,
                             const int32_t* lowAddr, const int32_t* uppAddr,

@@ -36,31 +36,85 @@ constexpr int kScratchDoubles = kMaxGroups + 32;  // + one 256-byte line for the
 // host it is only a stand-in for the symbol, not a device address (a kernel
 // given it would fault, or on systems where the GPU can reach host memory
 // silently use the wrong memory).  The device address comes from
-// cudaGetSymbolAddress, once per device (see scratch_for_current_device).
+// cudaGetSymbolAddress, once per CUDA context (see scratch_for_current_context).
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-double* g_scratchPtr[kMaxDevices] = {nullptr};
+// Device addresses of the array, one per CUDA context that has called.  An
+// address from cudaGetSymbolAddress belongs to the context current at the
+// lookup, so the key is that context (cuCtxGetCurrent, fetched through the
+// runtime's driver entry point so the library does not link libcuda): a
+// driver-API caller that makes another context current on the same device
+// gets its own lookup.
+struct ScratchEntry
+{
+    void* ctx;
+    double* ptr;
+};
+constexpr int kMaxEntries = 64;
+ScratchEntry g_scratch[kMaxEntries];
+int g_scratchCount = 0;
 std::mutex g_scratchMutex;
 
-int scratch_for_current_device(double** out)
+typedef int (*CtxGetCurrentFn)(void**);
+
+int current_context(void** out)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-        return cf::fail(CF_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    static CtxGetCurrentFn fn = nullptr;
+    static cudaError_t fnStatus = cudaErrorUnknown;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        fnStatus = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000,
+                                                    cudaEnableDefault, &q);
+        if (fnStatus == cudaSuccess && q == cudaDriverEntryPointSuccess && f)
+            fn = (CtxGetCurrentFn)f;
+        else if (fnStatus == cudaSuccess)
+            fnStatus = cudaErrorSymbolNotFound;
+    });
+    if (!fn)
+        return cf::fail(CF_ERR_CUDA, std::string("cuCtxGetCurrent entry point: ") +
+                                         cudaGetErrorString(fnStatus));
+    *out = nullptr;
+    if (fn(out) != 0 || !*out)
+        return cf::fail(CF_ERR_CUDA, "cuCtxGetCurrent: no current CUDA context");
+    return CF_OK;
+}
+
+// The scratch address for the current context.  The lookup itself is not a
+// stream operation but may load the module on first use, which a stream
+// capture in progress must not see: a first call on a context while `s` is
+// capturing is refused with a message saying so.
+int scratch_for_current_context(cudaStream_t s, double** out)
+{
+    // the capture query also initialises the runtime (and the primary
+    // context) on a thread whose first CUDA call this is
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t ce = cudaStreamIsCapturing(s, &cs);
+    if (ce != cudaSuccess) cudaGetLastError();
+    void* ctx = nullptr;
+    int rc = current_context(&ctx);
+    if (rc != CF_OK) return rc;
     std::lock_guard<std::mutex> lock(g_scratchMutex);
-    if (dev >= 0 && dev < kMaxDevices && g_scratchPtr[dev])
-    {
-        *out = g_scratchPtr[dev];
-        return CF_OK;
-    }
+    for (int i = 0; i < g_scratchCount; ++i)
+        if (g_scratch[i].ctx == ctx)
+        {
+            *out = g_scratch[i].ptr;
+            return CF_OK;
+        }
+    if (ce != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return cf::fail(CF_ERR_UNSUPPORTED,
+                        "cf_ldu_spmv_dot_noalloc: the first call in a CUDA context looks up the "
+                        "scratch array's device address and must be made outside stream capture; "
+                        "make one call (any size) before capturing");
+    if (g_scratchCount == kMaxEntries)
+        return cf::fail(CF_ERR_TOO_LARGE, "cf_ldu_spmv_dot_noalloc: more than 64 CUDA contexts");
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
         return cf::fail(CF_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
                                          cudaGetErrorString(e));
-    if (dev >= 0 && dev < kMaxDevices) g_scratchPtr[dev] = (double*)p;
+    g_scratch[g_scratchCount++] = {ctx, (double*)p};
     *out = (double*)p;
     return CF_OK;
 }
@@ -156,13 +210,16 @@ extern "C" int cf_ldu_spmv_dot_noalloc(int32_t nCells, const float* diag, const 
                         "cf_ldu_spmv_dot_noalloc: nCells " + std::to_string(nCells) +
                             " exceeds the fixed scratch limit of " +
                             std::to_string((long long)kMaxGroups * kBlock) + " cells");
-    if (!diag || !upper || !ownStartAddr || !losortStartAddr || !x || !y)
-        return cf::fail(CF_ERR_INVALID_ARG, "NULL device pointer");
+    // every addressing array is read for any row that has faces, so none
+    // may be NULL (a mesh without faces passes any valid device pointer)
+    if (!diag || !upper || !lowAddr || !uppAddr || !ownStartAddr || !losortAddr ||
+        !losortStartAddr || !x || !y)
+        return cf::fail(CF_ERR_INVALID_ARG, "cf_ldu_spmv_dot_noalloc: NULL device pointer");
     if (!lower) lower = upper;
-    double* scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
-    if (rc != CF_OK) return rc;
     cudaStream_t s = (cudaStream_t)stream;
+    double* scratch = nullptr;
+    int rc = scratch_for_current_context(s, &scratch);
+    if (rc != CF_OK) return rc;
     if (dot)
     {
         // the counter must start at zero; the array keeps the last call's

@@ -76,3 +76,28 @@ def test_solver_selection_and_errors():
     solver = lduMatrix.solver.New("p", sym, {"solver": "cudaPCG"}, interfaces=[object()])
     with pytest.raises(FatalError):
         solver.solve(np.zeros(s.n), s.source)
+
+
+def test_noalloc_rejects_null_pointers_before_any_device_work():
+    """cf_ldu_spmv_dot_noalloc checks its pointers on the host: a NULL
+    addressing array (read for every row with faces) or operand returns
+    CF_ERR_INVALID_ARG and launches nothing, so this runs without a GPU.
+    The pointer values below are never dereferenced."""
+    from metal4foam_b200 import _lib
+    L = _lib.load()
+    fake = 0x1000
+    args = [fake] * 9  # diag upper lower low upp ownStart losort losortStart x
+    names = ["diag", "upper", "lower", "lowAddr", "uppAddr", "ownStartAddr", "losortAddr",
+             "losortStartAddr", "x"]
+    for k, name in enumerate(names):
+        if name == "lower":   # NULL lower means symmetric
+            continue
+        a = list(args)
+        a[k] = None
+        rc = L.cf_ldu_spmv_dot_noalloc(10, *a, fake, fake, fake, None)
+        assert rc == 1, name
+        assert b"NULL" in L.cf_last_error(), name
+    rc = L.cf_ldu_spmv_dot_noalloc(10, *args, fake, None, fake, None)   # y NULL
+    assert rc == 1
+    rc = L.cf_ldu_spmv_dot_noalloc(0, *args, fake, fake, fake, None)
+    assert rc == 1

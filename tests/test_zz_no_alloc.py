@@ -4,8 +4,9 @@ threads that must not take the allocator's locks, or in frameworks that hand
 out only their own buffers).  Its output must equal the context entry point
 cf_spmv32 on the same FP32 operator: y bit for bit (same per-row order) and
 the dot within 1e-12 relative, on two calls in a row (the shared scratch and
-its completion counter are reused).  The test allocates its own buffers with
-torch; the entry point allocates none.  Collected last on purpose."""
+its completion counter are reused).  Without w the dot is 0; without dot
+only y is written.  The test allocates its own buffers with torch; the entry
+point allocates none.  Collected last on purpose."""
 import numpy as np
 import pytest
 
@@ -53,6 +54,39 @@ def test_noalloc_matches_context_spmv(require_gpu, kind):
         assert rc == 0, L.cf_last_error()
         assert np.array_equal(d_y.cpu().numpy(), y_ref), f"call {call}"
         assert d_dot.item() == pytest.approx(dot_ref, rel=1e-12, abs=1e-12), f"call {call}"
+
+    # w = NULL: y as before, the dot of nothing is exactly 0
+    d_y.fill_(float("nan"))
+    d_dot.fill_(float("nan"))
+    rc = L.cf_ldu_spmv_dot_noalloc(
+        s.n, _lib.ptr(d_diag), _lib.ptr(d_upper), _lib.ptr(d_lower),
+        *(_lib.ptr(t) for t in addr), _lib.ptr(d_x), None, _lib.ptr(d_y),
+        _lib.ptr(d_dot), _lib.vp(stream.cuda_stream))
+    torch.cuda.synchronize()
+    assert rc == 0, L.cf_last_error()
+    assert np.array_equal(d_y.cpu().numpy(), y_ref)
+    assert d_dot.item() == 0.0
+
+    # dot = NULL: y only; the dot buffer is left untouched
+    d_y.fill_(float("nan"))
+    d_dot.fill_(7.0)
+    rc = L.cf_ldu_spmv_dot_noalloc(
+        s.n, _lib.ptr(d_diag), _lib.ptr(d_upper), _lib.ptr(d_lower),
+        *(_lib.ptr(t) for t in addr), _lib.ptr(d_x), _lib.ptr(d_w), _lib.ptr(d_y),
+        None, _lib.vp(stream.cuda_stream))
+    torch.cuda.synchronize()
+    assert rc == 0, L.cf_last_error()
+    assert np.array_equal(d_y.cpu().numpy(), y_ref)
+    assert d_dot.item() == 7.0
+
+    # and a full call again after both: the shared counter is still sound
+    rc = L.cf_ldu_spmv_dot_noalloc(
+        s.n, _lib.ptr(d_diag), _lib.ptr(d_upper), _lib.ptr(d_lower),
+        *(_lib.ptr(t) for t in addr), _lib.ptr(d_x), _lib.ptr(d_w), _lib.ptr(d_y),
+        _lib.ptr(d_dot), _lib.vp(stream.cuda_stream))
+    torch.cuda.synchronize()
+    assert rc == 0, L.cf_last_error()
+    assert d_dot.item() == pytest.approx(dot_ref, rel=1e-12, abs=1e-12)
 
 
 def test_noalloc_rejects_sizes_beyond_scratch(require_gpu):
