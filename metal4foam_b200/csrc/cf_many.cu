@@ -33,6 +33,14 @@ extern "C" int cf_solve_many_device(cf_context* const* ctx, int32_t count, int32
         for (int k = 0; k < i; ++k)
             if (ctx[k] == ctx[i])
                 return fail(CF_ERR_INVALID_ARG, "a context appears twice (one system each)");
+    // the worker streams are created on one device and only that device is
+    // synchronised: every context must live there
+    for (int i = 1; i < count; ++i)
+        if (ctx[i]->device != ctx[0]->device)
+            return fail(CF_ERR_INVALID_ARG, "system " + std::to_string(i) + " is on device " +
+                                                std::to_string(ctx[i]->device) + ", system 0 on " +
+                                                std::to_string(ctx[0]->device) +
+                                                ": all contexts must share one device");
     if (count == 0) return CF_OK;
     // inputs produced by earlier work on any stream are complete
     {
