@@ -93,6 +93,23 @@ class TuneEntry(C.Structure):
     _fields_ = [("config", SpmvConfig), ("msPerLaunch", C.c_double)]
 
 
+class StepIO(C.Structure):
+    """cf_step_io: vectors of one fused inner-iteration kernel (cf_inner_step)."""
+    VECTORS = ["rA", "rA0", "wA", "pOld", "AyAOld", "delta", "zIn", "wIn", "p", "q", "yA",
+               "AyA", "sA", "zA", "tA", "deltaNext", "rAOut", "wAOut", "wOut", "zOut"]
+    _fields_ = ([(k, vp) for k in VECTORS] +
+                [("alpha", C.c_double), ("beta", C.c_double), ("omega", C.c_double),
+                 ("chebOrder", C.c_int32), ("chebStep", C.c_int32), ("chebBeta", C.c_double),
+                 ("chebRatio", C.c_double), ("sums", C.c_double * 3)])
+
+
+STEPS = {"cheb": 0, "pcg_p_spmv": 1, "pcg_update": 2, "bicg_ab": 3, "bicg_cd": 4, "bicg_e": 5}
+# vectors each step writes (the others it reads)
+STEP_OUTPUTS = {"cheb": ["wOut", "zOut"], "pcg_p_spmv": ["p", "q"],
+                "pcg_update": ["deltaNext", "rAOut", "wAOut"],
+                "bicg_ab": ["p", "yA", "AyA"], "bicg_cd": ["sA", "zA", "tA"],
+                "bicg_e": ["deltaNext", "rAOut"]}
+
 CF_LAYOUT_SELL32 = 0
 CF_LAYOUT_LDU = 1
 LAYOUTS = {"sell32": CF_LAYOUT_SELL32, "ldu": CF_LAYOUT_LDU}
@@ -115,6 +132,7 @@ SIGNATURES = [
     ("cf_context_set_stream", C.c_int, [vp, vp]),
     ("cf_context_set_reorder", C.c_int, [vp, i32]),
     ("cf_context_kernel_launches", C.c_int, [vp, C.POINTER(C.c_longlong)]),
+    ("cf_context_set_wait_limit", C.c_int, [vp, C.c_int64]),
     ("cf_set_topology", C.c_int, [vp, i32, i32, vp, vp, vp, vp, vp]),
     ("cf_set_coeffs", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
     ("cf_set_coeffs_device", C.c_int, [vp, vp, vp, vp]),
@@ -161,6 +179,7 @@ SIGNATURES = [
     ("cf_spmv32", C.c_int, [vp, vp, vp, vp, C.POINTER(dbl)]),
     ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
     ("cf_time_kernel", C.c_int, [vp, i32, i32, C.POINTER(dbl)]),
+    ("cf_inner_step", C.c_int, [vp, i32, C.POINTER(StepIO)]),
     ("cf_ldu_spmv_dot_noalloc", C.c_int, [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp]),
 ]
@@ -281,6 +300,9 @@ class Context:
         n = C.c_longlong()
         check(load().cf_context_kernel_launches(self.h, C.byref(n)))
         return n.value
+
+    def set_wait_limit(self, polls=0):
+        check(load().cf_context_set_wait_limit(self.h, int(polls)))
 
     def set_stream(self, stream_handle):
         check(load().cf_context_set_stream(self.h, vp(stream_handle) if stream_handle else None))
@@ -446,6 +468,29 @@ class Context:
                                  C.byref(count)))
         return best, [(table[i].config.as_dict(), table[i].msPerLaunch)
                       for i in range(min(count.value, 64))]
+
+    def inner_step(self, step, n, alpha=0.0, beta=0.0, omega=0.0, chebOrder=1, chebStep=0,
+                   chebBeta=2.0, chebRatio=30.0, **vectors):
+        """One launch of a fused inner-iteration kernel (cf_inner_step):
+        `vectors` are the step's FP32 inputs by name; returns (outputs by
+        name, sums)."""
+        io = StepIO()
+        keep = []
+        for k, v in vectors.items():
+            a = np.ascontiguousarray(v, np.float32)
+            keep.append(a)
+            setattr(io, k, a.ctypes.data)
+        outs = {}
+        for k in STEP_OUTPUTS[step]:
+            if k in vectors:     # an input the step also writes is not an output slot
+                continue
+            outs[k] = np.empty(n, np.float32)
+            setattr(io, k, outs[k].ctypes.data)
+        io.alpha, io.beta, io.omega = float(alpha), float(beta), float(omega)
+        io.chebOrder, io.chebStep = int(chebOrder), int(chebStep)
+        io.chebBeta, io.chebRatio = float(chebBeta), float(chebRatio)
+        check(load().cf_inner_step(self.h, STEPS[step], C.byref(io)))
+        return outs, list(io.sums)
 
     def cheb_apply(self, r, order, beta, ratio=30.0):
         rr = np.ascontiguousarray(r, np.float32)

@@ -92,8 +92,17 @@ def build():
     """Compile liboracle.so (and libmslref.so when the reference is here)."""
     import subprocess
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isdir(os.environ.get("REFERENCE_DIR", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref = reference_dir()
+    if os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_DIR={ref}"], check=True)
+
+
+def reference_dir():
+    """The reference checkout: $REFERENCE_DIR, else the directory
+    `reference` beside this repository's root (absent on machines that only
+    use the prebuilt oracle)."""
+    return os.environ.get("REFERENCE_DIR") or os.path.normpath(
+        os.path.join(HERE, "..", "..", "reference"))
 
 
 def lib():
@@ -394,3 +403,109 @@ class Ldu32View:
             lib().orc_k_ldu_spmv(C.byref(self.s), z, v)
             lib().orc_k_cheb_step(n, r, v, self.rD, w, z, c[2 * i - 1], c[2 * i])
         return z
+
+
+# ------------------------------------------- the reference's kernel sequences
+# Slots of the reference's scalar buffer (metalFoamKernels.metal:20-32).
+S_ALPHA, S_BETA, S_OMEGA, S_COUNT = 3, 4, 9, 16
+
+
+def _scalars(alpha=0.0, beta=0.0, omega=0.0):
+    s = np.zeros(S_COUNT, np.float32)
+    s[S_ALPHA], s[S_BETA], s[S_OMEGA] = alpha, beta, omega
+    return s
+
+
+def _group_count(n):
+    return max(1, (n + 255) // 256)
+
+
+class KernelSequence:
+    """One inner iteration's work as the reference dispatches it, kernel by
+    kernel (metalFoamBackend.C:608-906), on FP32 copies of a system: each
+    method restates what one fused CUDA kernel replaces, with the scalars
+    alpha, beta, omega rounded to FP32 as the reference holds them.  Returns
+    the vectors the unfused kernels write, plus the FP64 sum of the same FP32
+    products that the fused kernel's reduction folds."""
+
+    def __init__(self, sysm):
+        self.v = Ldu32View(sysm)
+        self.n = sysm.n
+
+    def _spmv(self, x):
+        y, _ = self.v.spmv(x)
+        return y
+
+    def cheb_step(self, zin, win, rA, order, step, beta, ratio=30.0):
+        """ldu_spmv + cheb_step (metalFoamKernels.metal:64-150,174-194)."""
+        c = cheb_constants(order, beta, ratio)
+        v = self._spmv(zin)
+        w, z = _f32(win).copy(), _f32(zin).copy()
+        lib().orc_k_cheb_step(self.n, _f32(rA), v, self.v.rD, w, z, c[2 * step - 1], c[2 * step])
+        dot = float(np.dot(z.astype(np.float64), _f32(rA).astype(np.float64)))
+        return {"wOut": w, "zOut": z}, [dot if step == order - 1 else 0.0, 0.0, 0.0]
+
+    def pcg_p_spmv(self, wA, pOld, beta):
+        """pcg_update_p + ldu_spmv_dotw (metalFoamKernels.metal:64-109,237-247)."""
+        p = _f32(pOld).copy()
+        lib().orc_k_pcg_update_p(self.n, p, _f32(wA), _scalars(beta=beta))
+        q = self._spmv(p)
+        return {"p": p, "q": q}, [float(np.dot(p.astype(np.float64), q.astype(np.float64))),
+                                  0.0, 0.0]
+
+    def pcg_update(self, delta, p, rA, q, alpha, chebOrder=1, chebBeta=2.0, chebRatio=30.0):
+        """pcg_update_sol_res, then the next apply: cheb_init (Chebyshev) or
+        pcg_precond_dot (Jacobi) (metalFoamKernels.metal:154-171,212-276)."""
+        d, r = _f32(delta).copy(), _f32(rA).copy()
+        part = np.zeros(_group_count(self.n), np.float32)
+        lib().orc_k_pcg_update_sol_res(self.n, d, r, _f32(p), _f32(q), _scalars(alpha=alpha),
+                                       part)
+        w = np.empty(self.n, np.float32)
+        if chebOrder > 1:
+            c = cheb_constants(chebOrder, chebBeta, chebRatio)
+            z = np.empty(self.n, np.float32)
+            lib().orc_k_cheb_init(self.n, r, self.v.rD, w, z, c[0])
+            dot = 0.0
+        else:
+            lib().orc_k_pcg_precond_dot(self.n, r, self.v.rD, w, part)
+            dot = float(np.dot(w.astype(np.float64), r.astype(np.float64)))
+        l1 = float(np.sum(np.abs(r.astype(np.float64))))
+        return {"deltaNext": d, "rAOut": r, "wAOut": w}, [l1, dot, 0.0]
+
+    def bicg_ab(self, rA, pOld, AyAOld, rA0, beta, omega):
+        """bicg_update_p, emul, ldu_spmv_dotw (metalFoamKernels.metal:64-109,
+        198-208,372-386)."""
+        p = _f32(pOld).copy()
+        lib().orc_k_bicg_update_p(self.n, p, _f32(rA), _f32(AyAOld),
+                                  _scalars(beta=beta, omega=omega))
+        y = np.empty(self.n, np.float32)
+        lib().orc_k_emul(self.n, self.v.rD, p, y)
+        v = self._spmv(y)
+        dot = float(np.dot(_f32(rA0).astype(np.float64), v.astype(np.float64)))
+        return {"p": p, "yA": y, "AyA": v}, [dot, 0.0, 0.0]
+
+    def bicg_cd(self, rA, AyA, alpha):
+        """bicg_s_res, emul, ldu_spmv_dotw, dot_partial (metalFoamKernels.metal:
+        64-109,198-208,390-412,280-295)."""
+        s = np.empty(self.n, np.float32)
+        part = np.zeros(_group_count(self.n), np.float32)
+        lib().orc_k_bicg_s_res(self.n, s, _f32(rA), _f32(AyA), _scalars(alpha=alpha), part)
+        z = np.empty(self.n, np.float32)
+        lib().orc_k_emul(self.n, self.v.rD, s, z)
+        t = self._spmv(z)
+        s64, t64 = s.astype(np.float64), t.astype(np.float64)
+        return {"sA": s, "zA": z, "tA": t}, [float(np.sum(np.abs(s64))), float(np.dot(s64, t64)),
+                                             float(np.dot(t64, t64))]
+
+    def bicg_e(self, delta, yA, zA, sA, tA, rA0, alpha, omega):
+        """bicg_update_sol_res + dot_partial of rA0.rA (metalFoamKernels.metal:
+        280-295,430-458)."""
+        d = _f32(delta).copy()
+        r = np.empty(self.n, np.float32)
+        part = np.zeros(_group_count(self.n), np.float32)
+        lib().orc_k_bicg_update_sol_res(self.n, d, _f32(yA), _f32(zA), r, _f32(sA), _f32(tA),
+                                        _scalars(alpha=alpha, omega=omega), part)
+        r64 = r.astype(np.float64)
+        return {"deltaNext": d, "rAOut": r}, [float(np.sum(np.abs(r64))),
+                                              float(np.dot(_f32(rA0).astype(np.float64), r64)),
+                                              0.0]
