@@ -523,6 +523,13 @@ extern "C" int cf_context_set_reorder(cf_context* c, int32_t mode)
     return CF_OK;
 }
 
+extern "C" int cf_context_set_wait_limit(cf_context* c, int64_t polls)
+{
+    if (!c || polls < 0) return fail(CF_ERR_INVALID_ARG, "bad wait limit");
+    c->waitPolls = polls == 0 ? (1LL << 24) : (long long)polls;
+    return CF_OK;
+}
+
 extern "C" int cf_context_kernel_launches(const cf_context* c, long long* count)
 {
     if (!c || !count) return fail(CF_ERR_INVALID_ARG, "NULL argument");

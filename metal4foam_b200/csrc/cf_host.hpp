@@ -116,6 +116,7 @@ struct cf_context
     int clusterShift = 10;                 // log2(rows per CTA) of the cluster PCG for this mesh
     double clusterRemote = 1.0;            // fraction of entries whose column lies in another CTA
     unsigned int* d_bar = nullptr;         // grid barrier of persistent inner solves: count, generation, error
+    long long waitPolls = 1LL << 24;       // polls of a bounded device-side wait before it gives up
     int cfgLayout = 0;
     int cfgRowsPerWarp = 32;
     int cfgBlockSize = 256;

@@ -18,10 +18,11 @@
 //
 // Grid barrier: generation counter in global memory; the last block to
 // arrive resets the count and bumps the generation.  Every wait is bounded
-// (kBarrierSpins polls with a short sleep); a block that gives up sets the
-// error word and leaves, the others leave at their next barrier, and the
-// host reports CF_ERR_DEVICE_TIMEOUT.  The launch is cooperative, so all
-// blocks are co-resident and the bound is never reached in normal runs.
+// (the context's wait limit, default 2^24 polls with a short sleep each,
+// cf_context_set_wait_limit); a block that gives up sets the error word and
+// leaves, the others leave at their next barrier, and the host reports
+// CF_ERR_DEVICE_TIMEOUT.  The launch is cooperative, so all blocks are
+// co-resident and the default bound is never reached in normal runs.
 //
 // Opt-in (cf_options.persistentMaxCells > 0, cudaPCG): measured on B200 it
 // is 20-35% slower than the graph-driven loop on 16k-64k-cell meshes (PCG,
@@ -39,7 +40,6 @@ using namespace cf;
 
 namespace {
 
-constexpr unsigned long long kBarrierSpins = 1ull << 24;
 constexpr int MW = MAXW_UNROLL;
 
 struct Bar
@@ -47,6 +47,7 @@ struct Bar
     unsigned int* count;
     unsigned int* gen;
     int* err;
+    unsigned long long polls;   // polls of one wait before it gives up
 };
 
 __device__ __forceinline__ bool grid_barrier(const Bar& b)
@@ -68,7 +69,7 @@ __device__ __forceinline__ bool grid_barrier(const Bar& b)
             unsigned long long spins = 0;
             while (*vgen == g)
             {
-                if (++spins > kBarrierSpins)
+                if (++spins > b.polls)
                 {
                     atomicExch(b.err, 1);
                     break;
@@ -253,7 +254,8 @@ int persistent_inner(cf_context* c, int kind, int order, int maxCells, bool* ran
     if (cudaMemsetAsync(c->d_bar, 0, sizeof(unsigned int) * 4, s) != cudaSuccess)
         return fail(CF_ERR_CUDA, "cudaMemsetAsync (grid barrier)");
     const DevSell A = sell_of(c);
-    Bar bar{c->d_bar, c->d_bar + 1, reinterpret_cast<int*>(c->d_bar + 2)};
+    Bar bar{c->d_bar, c->d_bar + 1, reinterpret_cast<int*>(c->d_bar + 2),
+            (unsigned long long)c->waitPolls};
     PcgBufs B = pcg_bufs(c);
     InnerState* st = c->d_st;
     double* part = c->d_part;

@@ -65,3 +65,32 @@ def test_persistent_not_used_above_limit(require_gpu):
     _, p1, l1 = run(s, _lib.CF_SOLVER_PCG, True, persistentMaxCells=1000)
     _, p2, l2 = run(s, _lib.CF_SOLVER_PCG, False)
     assert l1 == l2 and p1.nIterations == p2.nIterations
+
+
+def test_persistent_barrier_timeout_is_reported_and_context_recovers(require_gpu):
+    """Every grid-barrier wait of the persistent kernel is bounded.  With a
+    wait limit of one poll, a block that arrives first at a barrier gives
+    up before the other 249 blocks arrive: the kernel ends (every block
+    leaves at its next barrier), cf_solve returns CF_ERR_DEVICE_TIMEOUT,
+    and a following solve on the same context, with the default limit,
+    converges to what the graph loop returns."""
+    s = mesh.varcoeff3d((40, 40, 40), seed=4, permute=True)
+    ctx = _lib.Context(0)
+    a = s.addr
+    ctx.set_topology(a.n, a.nf, *a.arrays())
+    ctx.set_coeffs(s.diag, s.upper, None)
+    opts = _lib.default_options(persistentMaxCells=1 << 20, clusterMaxCells=-1)
+    ctx.set_wait_limit(1)
+    x = np.zeros(s.n)
+    with pytest.raises(_lib.CudaFoamError) as ei:
+        ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, opts)
+    assert ei.value.code == 7, str(ei.value)
+    ctx.set_wait_limit(0)
+    x = np.zeros(s.n)
+    p = ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, opts)
+    assert p.converged and p.finalResidual < 1e-6
+    ctx.close()
+    xg, pg, _ = run(s, _lib.CF_SOLVER_PCG, False)
+    assert np.array_equal(x, xg) and p.nIterations == pg.nIterations
+    with pytest.raises(_lib.CudaFoamError):
+        _lib.Context(0).set_wait_limit(-1)
