@@ -542,6 +542,77 @@ int cf_solve_many_device(cf_context* const* ctx, int32_t count, int32_t solver,
                          const double* const* lower, const cf_options* opts, int32_t streams,
                          cf_performance* perf);
 
+/* ------------------------------------------------------------ subdomains */
+/* A subdomain of a decomposed mesh solved together with its neighbours
+ * across processor interfaces.  The reference rejects coupled interfaces
+ * (metalFoamSolver.C:89-99); these entry points have no counterpart there.
+ * Each subdomain (one per MPI rank, GPU or thread) holds its own LDU matrix
+ * in the lduAddressing form of cf_set_topology plus nInterfaces processor
+ * interfaces in OpenFOAM's form: interface p faces subdomain neighbour[p];
+ * faceCells (nFaces[0] + nFaces[1] + ... entries, interface after
+ * interface) are this side's cells of the interface faces, listed in the
+ * same face order as the neighbour lists them; interfaceCoeffs (same
+ * layout) are the interfaceBouCoeffs: row faceCells[k] of A psi gets
+ * -interfaceCoeffs[k] * psi_neighbour[k], after the internal faces, as
+ * lduMatrix::Amul's updateMatrixInterfaces does.  At most one interface per
+ * neighbouring subdomain.
+ *
+ * Communication is the caller's (MPI/Pstream, NCCL, or the in-process hub
+ * of cf_comm_local_create).  Both callbacks receive device pointers on the
+ * subdomain's device and the subdomain's cudaStream_t; they may complete
+ * the work before returning or enqueue it on that stream (NCCL), as long as
+ * work enqueued on the stream afterwards sees the result.  They return 0 on
+ * success.  Every subdomain calls them in the same order with the same
+ * counts (all decisions depend on globally reduced values). */
+typedef struct cf_comm
+{
+    void* user;
+    /* in place over all subdomains: op 0 sum, 1 max, of `count` doubles */
+    int (*allreduce)(void* user, double* values, int32_t count, int32_t op, void* stream);
+    /* for every interface p: send[p] (nFaces[p] elements of elemBytes,
+     * this side's face order) to subdomain neighbour[p]; that subdomain's
+     * values for the same faces into recv[p] */
+    int (*exchange)(void* user, int32_t nInterfaces, const int32_t* neighbour,
+                    const int32_t* nFaces, int32_t elemBytes, const void* const* send,
+                    void* const* recv, void* stream);
+    /* optional: called when this subdomain's solve fails, so the others
+     * stop waiting for it */
+    void (*abort)(void* user);
+} cf_comm;
+
+typedef struct cf_subdomain cf_subdomain;
+
+int cf_subdomain_create(cf_subdomain** out, int32_t device);
+int cf_subdomain_destroy(cf_subdomain* sub);
+int cf_subdomain_set_stream(cf_subdomain* sub, void* stream);
+int cf_subdomain_kernel_launches(const cf_subdomain* sub, long long* count);
+/* internal addressing (validated as by cf_set_topology) and interfaces;
+ * reorder: CF_REORDER_* of the internal cells */
+int cf_subdomain_set_topology(cf_subdomain* sub, int32_t nCells, int32_t nFaces,
+                              const int32_t* lowAddr, const int32_t* uppAddr,
+                              const int32_t* ownStartAddr, const int32_t* losortAddr,
+                              const int32_t* losortStartAddr, int32_t nInterfaces,
+                              const int32_t* neighbour, const int32_t* nInterfaceFaces,
+                              const int32_t* faceCells, int32_t reorder);
+/* FP64 diag, upper, lower (NULL: symmetric) and interfaceCoeffs (host) */
+int cf_subdomain_set_coeffs(cf_subdomain* sub, const double* diag, const double* upper,
+                            const double* lower, const double* interfaceCoeffs);
+/* cf_solve's driver and inner solves over all subdomains (every sum global,
+ * halos exchanged before each SpMV; preconditioner Chebyshev-Jacobi; one
+ * host synchronisation per inner iteration); psi (in/out) and source are
+ * this subdomain's host arrays.  With no interfaces and one subdomain the
+ * result equals cf_solve's bit for bit. */
+int cf_subdomain_solve(cf_subdomain* sub, int32_t solver, double* psi, const double* source,
+                       const cf_options* opts, const cf_comm* comm, cf_performance* perf);
+
+/* An in-process communicator for nRanks subdomains solved by nRanks host
+ * threads of one process (one GPU or several): fills comms[0..nRanks-1].
+ * The threads meet at host barriers; a thread that waits longer than
+ * timeoutSeconds, or a failed solve (abort), makes every later call of
+ * every rank fail instead of waiting. */
+int cf_comm_local_create(int32_t nRanks, double timeoutSeconds, cf_comm* comms);
+int cf_comm_local_destroy(int32_t nRanks, cf_comm* comms);
+
 /* ------------------------------------------------------------ GAMG */
 /* Cells of every level of the context's multigrid hierarchy (built by the
  * first cudaPCG solve with CF_PRECOND_GAMG on the current topology; level 0

@@ -110,6 +110,17 @@ STEP_OUTPUTS = {"cheb": ["wOut", "zOut"], "pcg_p_spmv": ["p", "q"],
                 "bicg_ab": ["p", "yA", "AyA"], "bicg_cd": ["sA", "zA", "tA"],
                 "bicg_e": ["deltaNext", "rAOut"]}
 
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, vp, vp, C.c_int32, C.c_int32, vp)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, vp, C.c_int32, vp, vp, C.c_int32, vp, vp, vp)
+ABORT_FN = C.CFUNCTYPE(None, vp)
+
+
+class Comm(C.Structure):
+    """cf_comm: the subdomains' communication callbacks."""
+    _fields_ = [("user", vp), ("allreduce", ALLREDUCE_FN), ("exchange", EXCHANGE_FN),
+                ("abort", ABORT_FN)]
+
+
 CF_LAYOUT_SELL32 = 0
 CF_LAYOUT_LDU = 1
 LAYOUTS = {"sell32": CF_LAYOUT_SELL32, "ldu": CF_LAYOUT_LDU}
@@ -180,6 +191,17 @@ SIGNATURES = [
     ("cf_cheb_apply", C.c_int, [vp, vp, vp, i32, dbl, dbl]),
     ("cf_time_kernel", C.c_int, [vp, i32, i32, C.POINTER(dbl)]),
     ("cf_inner_step", C.c_int, [vp, i32, C.POINTER(StepIO)]),
+    ("cf_subdomain_create", C.c_int, [C.POINTER(vp), i32]),
+    ("cf_subdomain_destroy", C.c_int, [vp]),
+    ("cf_subdomain_set_stream", C.c_int, [vp, vp]),
+    ("cf_subdomain_kernel_launches", C.c_int, [vp, C.POINTER(C.c_longlong)]),
+    ("cf_subdomain_set_topology", C.c_int, [vp, i32, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp,
+                                            i32]),
+    ("cf_subdomain_set_coeffs", C.c_int, [vp, vp, vp, vp, vp]),
+    ("cf_subdomain_solve", C.c_int, [vp, i32, vp, vp, C.POINTER(Options), C.POINTER(Comm),
+                                     C.POINTER(Performance)]),
+    ("cf_comm_local_create", C.c_int, [i32, C.c_double, C.POINTER(Comm)]),
+    ("cf_comm_local_destroy", C.c_int, [i32, C.POINTER(Comm)]),
     ("cf_ldu_spmv_dot_noalloc", C.c_int, [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp]),
 ]
@@ -562,3 +584,83 @@ class Batch:
 
     def solve_device(self, psis, sources, options):
         return self._solve(load().cf_batch_solve_device, psis, sources, options)
+
+
+class SubdomainSolver:
+    """One subdomain of a decomposed system (cf_subdomain_*): its internal
+    LDU matrix plus processor interfaces (metal4foam_b200.decompose)."""
+
+    def __init__(self, sub, device: int = 0, reorder: str = "auto"):
+        L = load()
+        h = vp()
+        check(L.cf_subdomain_create(C.byref(h), int(device)))
+        self.h = h
+        self.sub = sub
+        s = sub.system
+        a = s.addr
+        nb, nfc, fc, cf = sub.interface_arrays()
+        self._keep = (a.arrays(), nb, nfc, fc)
+        check(L.cf_subdomain_set_topology(self.h, a.n, a.nf, *(ptr(x) for x in a.arrays()),
+                                          len(nb), ptr(nb), ptr(nfc), ptr(fc), REORDER[reorder]))
+        self.set_coeffs(s.diag, s.upper, s.lower, cf)
+
+    def set_coeffs(self, diag, upper, lower, interfaceCoeffs):
+        d = np.ascontiguousarray(diag, np.float64)
+        u = np.ascontiguousarray(upper, np.float64)
+        lo = None if lower is None else np.ascontiguousarray(lower, np.float64)
+        c = np.ascontiguousarray(interfaceCoeffs, np.float64)
+        check(load().cf_subdomain_set_coeffs(self.h, ptr(d), ptr(u), ptr(lo), ptr(c)))
+
+    def set_stream(self, stream_handle):
+        check(load().cf_subdomain_set_stream(self.h, vp(stream_handle) if stream_handle else None))
+
+    def solve(self, solver, psi, source, options, comm):
+        """psi (float64, this subdomain's cells) is updated in place; comm is
+        a Comm structure; returns the Performance (raises on failure)."""
+        assert psi.dtype == np.float64 and psi.flags.c_contiguous
+        src = np.ascontiguousarray(source, np.float64)
+        perf = Performance()
+        rc = load().cf_subdomain_solve(self.h, int(solver), ptr(psi), ptr(src),
+                                       C.byref(options), C.byref(comm), C.byref(perf))
+        check(rc)
+        return perf
+
+    def kernel_launches(self):
+        n = C.c_longlong()
+        check(load().cf_subdomain_kernel_launches(self.h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().cf_subdomain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LocalComm:
+    """The in-process communicator of cf_comm_local_create: nRanks Comm
+    structures for nRanks threads of this process."""
+
+    def __init__(self, nRanks: int, timeoutSeconds: float = 120.0):
+        self.n = int(nRanks)
+        self.comms = (Comm * self.n)()
+        check(load().cf_comm_local_create(self.n, float(timeoutSeconds), self.comms))
+
+    def __getitem__(self, r):
+        return self.comms[r]
+
+    def close(self):
+        if getattr(self, "comms", None) is not None:
+            load().cf_comm_local_destroy(self.n, self.comms)
+            self.comms = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

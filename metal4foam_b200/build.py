@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcudafoam.so")
 SOURCES = ["cf_context.cu", "cf_solve.cu", "cf_batched.cu", "cf_adjoint.cu", "cf_static.cu",
            "cf_multi.cu", "cf_tune.cu",
-           "cf_persist.cu", "cf_cluster.cu", "cf_amg.cu", "cf_many.cu", "cf_check.cu"]
+           "cf_persist.cu", "cf_cluster.cu", "cf_amg.cu", "cf_many.cu", "cf_check.cu",
+           "cf_coupled.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -232,9 +232,13 @@ int check_addressing(int32_t n, int32_t nf, const int32_t* low, const int32_t* u
 // Internal ordering + SELL-32 layout of one mesh on the host.
 int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
                  const int32_t* own, const int32_t* los, const int32_t* losS, bool rcm,
-                 HostLayout& L)
+                 HostLayout& L, const int32_t* xStart, const int32_t* xCol,
+                 const int32_t* xFace)
 {
     (void)nf;
+    // extra entries of cell i (xStart[i] .. xStart[i+1]) follow its losort
+    // faces; their columns are already internal (not relabelled)
+    auto nExtra = [&](int32_t i) { return xStart ? xStart[i + 1] - xStart[i] : 0; };
     std::vector<int32_t>& perm = L.perm;
     perm.clear();
     if (rcm) rcm_order(n, low, upp, own, los, losS, perm);
@@ -259,7 +263,7 @@ int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
             const int32_t r = s * SLICE + l;
             if (r >= n) break;
             const int32_t i = perm[r];
-            w = std::max(w, (own[i + 1] - own[i]) + (losS[i + 1] - losS[i]));
+            w = std::max(w, (own[i + 1] - own[i]) + (losS[i + 1] - losS[i]) + nExtra(i));
         }
         sw[s] = w;
         nnzSell += (long long)w * SLICE;
@@ -303,6 +307,12 @@ int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
             const size_t e = (size_t)L.sliceOff[s] + (size_t)SLICE * k + lane;
             L.col[e] = (int32_t)((uint32_t)iperm[low[f]] | 0x80000000u);
             L.eface[e] = f;
+        }
+        for (int32_t x = 0; x < nExtra(i); ++x, ++k)
+        {
+            const size_t e = (size_t)L.sliceOff[s] + (size_t)SLICE * k + lane;
+            L.col[e] = xCol[xStart[i] + x];
+            L.eface[e] = xFace[xStart[i] + x];
         }
         maxw = std::max(maxw, k);
     }

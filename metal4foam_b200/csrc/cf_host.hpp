@@ -153,9 +153,13 @@ struct HostLayout
 
 int check_addressing(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
                      const int32_t* own, const int32_t* los, const int32_t* losS);
+// xStart/xCol/xFace (optional, CSR over the caller's cells): extra entries
+// appended to a row after its losort faces, with internal columns xCol and
+// face indices xFace (processor-interface faces of a subdomain)
 int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
                  const int32_t* own, const int32_t* los, const int32_t* losS, bool rcm,
-                 HostLayout& L);
+                 HostLayout& L, const int32_t* xStart = nullptr, const int32_t* xCol = nullptr,
+                 const int32_t* xFace = nullptr);
 
 int fail(int code, const std::string& msg);
 double wall_now();
