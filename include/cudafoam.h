@@ -108,8 +108,11 @@ typedef struct
                                   cooperative kernel (grid barriers between
                                   the phases of an iteration, bit-identical
                                   results; slower than the graph loop on
-                                  B200, kept for comparison); 0 (default):
-                                  never                                    */
+                                  B200, kept for comparison); for a batch
+                                  (cf_batch_solve) whose rows all together
+                                  are at most this many, the inner loop of
+                                  every system runs as one cooperative
+                                  launch per restart; 0 (default): never   */
     int32_t clusterMaxCells;   /* cudaPCG with graph = 1: meshes up to this
                                   many cells (at most 16384, one row per
                                   thread) whose columns lie mostly in their
