@@ -580,6 +580,197 @@ __global__ void __launch_bounds__(1024) kb_compact(BArgs B, int force)
     }
 }
 
+// ------------------------------------------------ one persistent launch
+//
+// The inner loop of every system of the batch as ONE cooperative kernel:
+// the phases of an iteration (Chebyshev steps, p-update SpMV, update) over
+// the active tiles, separated by bounded grid barriers, then block 0
+// rebuilds the active-tile list -- what the graph loop's kernels do, in the
+// same per-row arithmetic and the same per-tile partial sums folded in tile
+// order, so every system gets bit for bit what the graph loop gives it.
+// Inside one launch L1 is not coherent across SMs: every load of data that
+// another block writes during the launch (vectors, partials, states, the
+// tile list) bypasses L1 (ld.global.cg, volatile); the matrix, diagonals,
+// constants and the tile table keep the read-only path.
+
+__device__ __forceinline__ float ldv(const float* p) { return __ldcg(p); }
+
+#define CFBP_ACTIVE_BEGIN(t)                                          \
+    const int nAct_ = *(volatile int*)&B.counters[2];                 \
+    for (int k_ = blockIdx.x; k_ < nAct_; k_ += gridDim.x)            \
+    {                                                                 \
+        const int t = __ldcg(B.actTiles + k_);                        \
+        const int s = __ldg(&B.tiles[t].x);                           \
+        const int tileRow = __ldg(&B.tiles[t].y);                     \
+        const BSys sy = B.sys[s];                                     \
+        const int tileEnd = min(tileRow + kTileRows, sy.row0 + sy.n); \
+        volatile InnerState* vq = B.st + s;
+
+template <bool LAST, int MAXW>
+__device__ __forceinline__ void kbp_cheb_step(const BArgs& B, const float* zin, const float* win,
+                                              float* wout, float* zout, int j)
+{
+    CFBP_ACTIVE_BEGIN(t)
+    if (vq->done) continue;
+    const float* cc = B.chebC + (size_t)s * kChebStride;
+    const float c2 = __ldg(cc + 2 * j - 1);
+    const float c3 = __ldg(cc + 2 * j);
+    double acc[1] = {0.0};
+    CFB_ROWS
+    {
+        const float zr = ldv(zin + row);
+        const float v = row_f32<MAXW>(B.A, row, __fmul_rn(__ldg(B.diag32 + row), zr),
+                                      [&](int c) { return ldv(zin + c); });
+        const float r = ldv(B.rA + row);
+        const float wn = __fadd_rn(__fmul_rn(c2, ldv(win + row)),
+                                   __fmul_rn(__fmul_rn(c3, __ldg(B.rD + row)), __fsub_rn(r, v)));
+        const float zn = __fadd_rn(zr, wn);
+        wout[row] = wn;
+        zout[row] = zn;
+        if (LAST) acc[0] += (double)zn * (double)r;
+    }
+    if (LAST)
+    {
+        if (sys_sum<1>(acc, B, t, s, &B.st[s].ticket) && threadIdx.x == 0)
+        {
+            vq->wArAold = vq->wArA;
+            vq->wArA = acc[0];
+            vq->beta = (vq->it == 0) ? 0.0 : vq->wArA / vq->wArAold;
+        }
+    }
+    CFB_TILE_END
+}
+
+template <int MAXW>
+__device__ __forceinline__ void kbp_pcg_p_spmv(const BArgs& B, const float* wA)
+{
+    CFBP_ACTIVE_BEGIN(t)
+    if (vq->done) continue;
+    const int par = vq->it & 1;
+    const float* Pold = B.P + (size_t)(par ^ 1) * B.N;
+    float* Pn = B.P + (size_t)par * B.N;
+    const float beta = (float)vq->beta;
+    double acc[1] = {0.0};
+    CFB_ROWS
+    {
+        auto pf = [&](int c) { return __fadd_rn(ldv(wA + c), __fmul_rn(beta, ldv(Pold + c))); };
+        const float pr = pf(row);
+        const float y = row_f32<MAXW>(B.A, row, __fmul_rn(__ldg(B.diag32 + row), pr), pf);
+        Pn[row] = pr;
+        B.Q[row] = y;
+        acc[0] += (double)pr * (double)y;
+    }
+    if (sys_sum<1>(acc, B, t, s, &B.st[s].ticket) && threadIdx.x == 0)
+    {
+        vq->wApA = acc[0];
+        vq->alpha = vq->wArA / vq->wApA;
+    }
+    CFB_TILE_END
+}
+
+template <bool CHEB>
+__device__ __forceinline__ void kbp_pcg_update(const BArgs& B)
+{
+    CFBP_ACTIVE_BEGIN(t)
+    if (vq->done) continue;
+    const int par = vq->it & 1;
+    const float* Pv = B.P + (size_t)par * B.N;
+    const float* Dc = B.D + (size_t)vq->cur * B.N;
+    float* Dn = B.D + (size_t)vq->nxt * B.N;
+    const float alpha = (float)vq->alpha;
+    const float c1 = CHEB ? __ldg(B.chebC + (size_t)s * kChebStride) : 0.0f;
+    double acc[2] = {0.0, 0.0};
+    CFB_ROWS
+    {
+        Dn[row] = __fadd_rn(ldv(Dc + row), __fmul_rn(alpha, ldv(Pv + row)));
+        const float rn = __fsub_rn(ldv(B.rA + row), __fmul_rn(alpha, ldv(B.Q + row)));
+        B.rA[row] = rn;
+        acc[0] += (double)fabsf(rn);
+        if (CHEB)
+        {
+            B.W0[row] = __fmul_rn(__fmul_rn(c1, __ldg(B.rD + row)), rn);
+        }
+        else
+        {
+            const float wa = __fmul_rn(rn, __ldg(B.rD + row));
+            B.W0[row] = wa;
+            acc[1] += (double)wa * (double)rn;
+        }
+    }
+    if (sys_sum<2>(acc, B, t, s, &B.st[s].ticket) && threadIdx.x == 0)
+    {
+        vq->res = acc[0];
+        if (!CHEB)
+        {
+            vq->wArAold = vq->wArA;
+            vq->wArA = acc[1];
+            vq->beta = vq->wArA / vq->wArAold;
+        }
+        vq->cur = vq->nxt;
+        vq->it = vq->it + 1;
+        inner_sync_point(vq, true);
+        if (vq->done)
+        {
+            *(volatile int*)&B.counters[3] = 1;
+            atomicSub(&B.counters[0], 1);
+        }
+    }
+    CFB_TILE_END
+}
+
+// kb_compact inside the persistent launch (block 0, NT threads)
+__device__ __forceinline__ void kbp_compact(const BArgs& B)
+{
+    __shared__ int count;
+    if (*(volatile int*)&B.counters[3] == 0) return;
+    if (threadIdx.x == 0) count = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < B.nTiles; t += NT)
+    {
+        const int s = __ldg(&B.tiles[t].x);
+        if (!((volatile InnerState*)(B.st + s))->done) B.actTiles[atomicAdd(&count, 1)] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        *(volatile int*)&B.counters[2] = count;
+        *(volatile int*)&B.counters[3] = 0;
+    }
+    __syncthreads();
+}
+
+template <bool CHEB, int MAXW>
+__global__ void __launch_bounds__(NT) kbp_pcg(BArgs B, int order, GridBar bar)
+{
+    float* Z[2] = {B.Z0, B.Z1};
+    // counters[0] (systems still iterating) changes only in the update
+    // phase; every block reads it after the same barrier
+    while (*(volatile int*)&B.counters[0] > 0)
+    {
+        const float* wA = B.W0;
+        if (CHEB)
+        {
+            for (int j = 1; j < order; ++j)
+            {
+                const float* zin = (j == 1) ? B.W0 : Z[(j - 1) & 1];
+                const float* win = (j == 1) ? B.W0 : B.W1;
+                if (j == order - 1)
+                    kbp_cheb_step<true, MAXW>(B, zin, win, B.W1, Z[j & 1], j);
+                else
+                    kbp_cheb_step<false, MAXW>(B, zin, win, B.W1, Z[j & 1], j);
+                if (!grid_barrier(bar)) return;
+            }
+            wA = Z[(order - 1) & 1];
+        }
+        kbp_pcg_p_spmv<MAXW>(B, wA);
+        if (!grid_barrier(bar)) return;
+        kbp_pcg_update<CHEB>(B);
+        if (!grid_barrier(bar)) return;
+        if (blockIdx.x == 0) kbp_compact(B);
+        if (!grid_barrier(bar)) return;
+    }
+}
+
 __global__ void kb_inner_final(int S, InnerState* st, BDrv* drv)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -781,6 +972,7 @@ struct cf_batch
     int2* d_tiles = nullptr;
     int* d_sliceOff = nullptr;
     int* d_col = nullptr;
+    short* d_col16 = nullptr;   // row-relative 16-bit columns for the FP32 kernels, or null
     int* d_eface = nullptr;
     int* d_perm = nullptr;
     double *d_upper = nullptr, *d_diagIn = nullptr, *d_diag64 = nullptr, *d_u = nullptr;
@@ -797,6 +989,8 @@ struct cf_batch
     double* d_part = nullptr;
     int* d_counters = nullptr;
     int* d_actTiles = nullptr;
+    unsigned int* d_bar = nullptr;   // grid barrier of the persistent loop: count, gen, error
+    bool coop = false;               // device supports cooperative launches
     BDrv* h_drv = nullptr;
     InnerState* h_st = nullptr;
     int* h_counters = nullptr;
@@ -873,6 +1067,7 @@ BArgs bargs(const cf_batch* bt)
     B.A.nslices = bt->nslices;
     B.A.sliceOff = bt->d_sliceOff;
     B.A.col = bt->d_col;
+    B.A.col16 = bt->d_col16;
     B.A.val = bt->d_val32;
     B.A.val64 = bt->d_val64;
     B.N = bt->N;
@@ -1043,6 +1238,40 @@ int fetch_counters(cf_batch* bt)
     return CF_OK;
 }
 
+// The inner loop of all systems as one cooperative launch (kbp_pcg) when
+// the device supports it; *ran tells whether it ran.  Waits for the launch
+// and reports a grid barrier that gave up as CF_ERR_DEVICE_TIMEOUT.
+int persistent_loop(cf_batch* bt, int order, bool* ran)
+{
+    *ran = false;
+    if (!bt->coop) return CF_OK;
+    const void* fn = order > 1 ? (const void*)kbp_pcg<true, MW> : (const void*)kbp_pcg<false, MW>;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, 0) != cudaSuccess || occ < 1)
+    {
+        cudaGetLastError();
+        return CF_OK;
+    }
+    const int grid = (int)std::max(1LL, std::min((long long)occ * bt->numSMs,
+                                                 (long long)bt->nTiles));
+    cudaStream_t s = bt->stream;
+    CFB_CUDA(cudaMemsetAsync(bt->d_bar, 0, sizeof(unsigned int) * 4, s));
+    BArgs B = bargs(bt);
+    GridBar bar{bt->d_bar, bt->d_bar + 1, reinterpret_cast<int*>(bt->d_bar + 2), 1ull << 24};
+    int ord = order;
+    void* args[] = {(void*)&B, (void*)&ord, (void*)&bar};
+    const cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), args, 0, s);
+    if (e != cudaSuccess)
+        return fail(CF_ERR_CUDA, std::string("cudaLaunchCooperativeKernel: ") + cudaGetErrorString(e));
+    bt->launches++;
+    int err = 0;
+    CFB_CUDA(cudaMemcpyAsync(&err, bt->d_bar + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CFB_CUDA(cudaStreamSynchronize(s));
+    if (err) return fail(CF_ERR_DEVICE_TIMEOUT, "a grid barrier of the persistent batched loop timed out");
+    *ran = true;
+    return CF_OK;
+}
+
 int batch_solve(cf_batch* bt, double* const* psi, const double* const* src, bool hostPtrs,
                 const cf_options* o, cf_performance* perf)
 {
@@ -1106,13 +1335,17 @@ int batch_solve(cf_batch* bt, double* const* psi, const double* const* src, bool
         CFB_TRY(fetch_counters(bt));
         if (bt->h_counters[0] > 0)
         {
-            if (o->graph)
+            // opt-in: the whole inner loop of all systems as one launch
+            bool ran = false;
+            if (o->graph && o->persistentMaxCells > 0 && bt->N <= o->persistentMaxCells)
+                CFB_TRY(persistent_loop(bt, order, &ran));
+            if (!ran && o->graph)
             {
                 cudaGraphExec_t exec;
                 CFB_TRY(batch_graph(bt, order, &exec));
                 CFB_CUDA(cudaGraphLaunch(exec, s));
             }
-            else
+            else if (!ran)
             {
                 for (int it = 0; it < o->maxIter; ++it)
                 {
@@ -1218,6 +1451,7 @@ extern "C" int cf_batch_create(cf_batch** out, int32_t device)
     bt->device = device;
     bt->numSMs = prop.multiProcessorCount;
     bt->maxBlocksPerSM = std::max(1, prop.maxThreadsPerMultiProcessor / NT);
+    bt->coop = prop.cooperativeLaunch != 0;
     if (cudaStreamCreateWithFlags(&bt->ownStream, cudaStreamNonBlocking) != cudaSuccess)
     {
         delete bt;
@@ -1342,6 +1576,34 @@ extern "C" int cf_batch_finalize(cf_batch* bt, int32_t reorder)
         for (int32_t r = 0; r < y.n; ++r) perm[y.row0 + r] = y.row0 + y.L.perm[r];
     }
     sliceOff[slices] = (int32_t)ent;
+    // compact column stream of the FP32 kernels (as for one system: the same
+    // columns as row-relative 16-bit offsets, when every system's columns lie
+    // within 32767 rows of their row; each system starts on a slice boundary,
+    // so slice k of the concatenation holds global rows 32 k .. 32 k + 31)
+    std::vector<short> col16;
+    {
+        bool fits = true;
+        std::vector<short> c16((size_t)std::max(ent, 1LL), COL16_PAD);
+        for (int k = 0; k < slices && fits; ++k)
+        {
+            const int32_t w = (sliceOff[k + 1] - sliceOff[k]) / SLICE;
+            for (int32_t j = 0; j < w && fits; ++j)
+                for (int32_t l = 0; l < SLICE; ++l)
+                {
+                    const long long e = (long long)sliceOff[k] + (long long)SLICE * j + l;
+                    if (col[e] == -1) continue;
+                    const long long off = (long long)((uint32_t)col[e] & 0x7fffffffu) -
+                                          ((long long)k * SLICE + l);
+                    if (off < -32767 || off > 32767)
+                    {
+                        fits = false;
+                        break;
+                    }
+                    c16[e] = (short)off;
+                }
+        }
+        if (fits) col16.swap(c16);
+    }
     const size_t N = (size_t)row;
     CFB_TRY(balloc(bt, &bt->d_sys, bt->S));
     CFB_TRY(balloc(bt, &bt->d_tiles, (size_t)tile));
@@ -1377,6 +1639,7 @@ extern "C" int cf_batch_finalize(cf_batch* bt, int32_t reorder)
     CFB_TRY(balloc(bt, &bt->d_part, (size_t)NPART * tile));
     CFB_TRY(balloc(bt, &bt->d_counters, 4));
     CFB_TRY(balloc(bt, &bt->d_actTiles, (size_t)tile));
+    CFB_TRY(balloc(bt, &bt->d_bar, 4));
     CFB_CUDA(cudaMallocHost((void**)&bt->h_drv, sizeof(BDrv) * bt->S));
     CFB_CUDA(cudaMallocHost((void**)&bt->h_st, sizeof(InnerState) * bt->S));
     CFB_CUDA(cudaMallocHost((void**)&bt->h_counters, 4 * sizeof(int)));
@@ -1387,6 +1650,12 @@ extern "C" int cf_batch_finalize(cf_batch* bt, int32_t reorder)
                              cudaMemcpyHostToDevice, s));
     CFB_CUDA(cudaMemcpyAsync(bt->d_col, col.data(), sizeof(int32_t) * col.size(),
                              cudaMemcpyHostToDevice, s));
+    if (!col16.empty())
+    {
+        CFB_TRY(balloc(bt, &bt->d_col16, col16.size()));
+        CFB_CUDA(cudaMemcpyAsync(bt->d_col16, col16.data(), sizeof(short) * col16.size(),
+                                 cudaMemcpyHostToDevice, s));
+    }
     CFB_CUDA(cudaMemcpyAsync(bt->d_eface, eface.data(), sizeof(int32_t) * eface.size(),
                              cudaMemcpyHostToDevice, s));
     CFB_CUDA(cudaMemcpyAsync(bt->d_perm, perm.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));

@@ -172,6 +172,53 @@ __device__ __forceinline__ bool grid_max(double& v, double* part,
     return true;
 }
 
+// Bounded grid barrier of a cooperative (all blocks co-resident) launch:
+// generation counter in global memory, the last block to arrive resets the
+// count and bumps the generation.  A block that has polled `polls` times
+// gives up: it sets the error word and the barrier returns false in every
+// block that sees it, so the kernel ends instead of waiting (the host then
+// reports CF_ERR_DEVICE_TIMEOUT).
+struct GridBar
+{
+    unsigned int* count;
+    unsigned int* gen;
+    int* err;
+    unsigned long long polls;
+};
+
+__device__ __forceinline__ bool grid_barrier(const GridBar& b)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned int* vgen = b.gen;
+        const unsigned int g = *vgen;
+        __threadfence();
+        if (atomicAdd(b.count, 1u) == gridDim.x - 1)
+        {
+            *b.count = 0u;
+            __threadfence();
+            atomicAdd(b.gen, 1u);
+        }
+        else
+        {
+            unsigned long long spins = 0;
+            while (*vgen == g)
+            {
+                if (++spins > b.polls)
+                {
+                    atomicExch(b.err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int*)b.err == 0;
+}
+
 __device__ __forceinline__ int free_buffer(int a, int b)
 {
     for (int i = 0; i < 3; ++i)

@@ -42,46 +42,7 @@ namespace {
 
 constexpr int MW = MAXW_UNROLL;
 
-struct Bar
-{
-    unsigned int* count;
-    unsigned int* gen;
-    int* err;
-    unsigned long long polls;   // polls of one wait before it gives up
-};
-
-__device__ __forceinline__ bool grid_barrier(const Bar& b)
-{
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        volatile unsigned int* vgen = b.gen;
-        const unsigned int g = *vgen;
-        __threadfence();
-        if (atomicAdd(b.count, 1u) == gridDim.x - 1)
-        {
-            *b.count = 0u;
-            __threadfence();
-            atomicAdd(b.gen, 1u);
-        }
-        else
-        {
-            unsigned long long spins = 0;
-            while (*vgen == g)
-            {
-                if (++spins > b.polls)
-                {
-                    atomicExch(b.err, 1);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return *(volatile int*)b.err == 0;
-}
+using Bar = GridBar;   // cf_kernels.cuh
 
 __device__ __forceinline__ float ld(const float* p) { return __ldcg(p); }
 

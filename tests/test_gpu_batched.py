@@ -139,3 +139,29 @@ def test_c4_batch_48_systems(require_gpu):
         r = s.source - mesh.amul_numpy(s, psi)
         assert np.sum(np.abs(r)) / p.normFactor < 1.01e-6
     bt.close()
+
+
+@pytest.mark.parametrize("order", [8, 1])
+def test_batch_one_persistent_launch_bitwise(require_gpu, order):
+    """Opt-in (persistentMaxCells >= the batch's rows): the inner loop of
+    every system runs as ONE cooperative launch per restart with bounded
+    grid barriers between the phases; every system gets bit for bit what
+    the graph loop gives it."""
+    systems = small_systems()
+    src = [s.source for s in systems]
+    bt = make_batch(systems)
+    base = dict(chebyshevOrder=order, maxRestarts=8, maxIter=3000)
+    a = [np.zeros(s.n) for s in systems]
+    l0 = bt.kernel_launches()
+    pa = bt.solve(a, src, _lib.default_options(**base))
+    la = bt.kernel_launches() - l0
+    b = [np.zeros(s.n) for s in systems]
+    l0 = bt.kernel_launches()
+    pb = bt.solve(b, src, _lib.default_options(persistentMaxCells=1 << 30, **base))
+    lb = bt.kernel_launches() - l0
+    for x, y, p, q in zip(a, b, pa, pb):
+        assert np.array_equal(x, y)
+        for f in ("nIterations", "nRestarts", "finalResidual", "converged", "deflated"):
+            assert getattr(p, f) == getattr(q, f), f
+    assert lb <= la, (lb, la)     # one launch per restart instead of one graph launch
+    bt.close()
