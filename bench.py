@@ -310,6 +310,16 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
 
     batched()
     ms_b = timed(batched, steps) / steps
+    res_graph = res["b"]
+    # the same batch with the inner loop of all systems in one persistent
+    # (cooperative) launch per restart
+    o_graph = o
+    o = _lib.default_options(persistentMaxCells=1 << 30, **opts)
+    batched()
+    res_persist = res["b"]
+    ms_bp = timed(batched, steps) / steps
+    o = o_graph
+    res["b"] = res_graph
     ctxs = []
     for s in loc:
         c = _lib.Context(local)
@@ -395,6 +405,15 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
             "plain_loop_solves_per_s": round(S / (ms_p / 1e3), 2),
             "host_sync_loop_solves_per_s": round(S / (ms_h / 1e3), 2),
             "speedup_vs_plain_loop": round(ms_p / ms_b, 3),
+            "persistent_launch": {
+                "note": "the batched solve with the inner loop of all systems as one "
+                        "cooperative launch per restart (persistentMaxCells), bounded grid "
+                        "barriers between phases; results bit-identical to the graph loop",
+                "ms": round(ms_bp, 2), "solves_per_s": round(S / (ms_bp / 1e3), 2),
+                "speedup_vs_plain_loop": round(ms_p / ms_bp, 3),
+                "speedup_vs_host_sync_loop": round(ms_h / ms_bp, 3),
+                "iterations_identical": [p.nIterations for p in res_persist] ==
+                                        [p.nIterations for p in res_graph]},
             "speedup_vs_host_sync_loop": round(ms_h / ms_b, 3),
             "ms": {"batched": round(ms_b, 2), "plain": round(ms_p, 2),
                    "host_sync": round(ms_h, 2)},
@@ -518,7 +537,7 @@ def run_gamg(ctx, d_diag, d_upper, d_src, stream, ms_reference, steps=5):
             "levels": ctx.gamg_levels(), "first_solve_s_with_hierarchy_build": round(first_s, 3)}
 
 
-def run_multi_rhs(local, stream, steps=3):
+def run_multi_rhs(local, stream, steps=3, dims=(64, 64, 64)):
     """One 64^3 upwind momentum matrix with 3 right-hand sides (Ux, Uy, Uz):
     cf_solve_multi (matrix read once per SpMV for all components) vs three
     cf_solve calls in sequence, inputs resident, same options (tolerance
@@ -527,7 +546,7 @@ def run_multi_rhs(local, stream, steps=3):
 
     from metal4foam_b200 import _lib, mesh
     dev = torch.device("cuda", local)
-    s, rhs = mesh.momentum_multi_rhs()
+    s, rhs = mesh.momentum_multi_rhs(dims)
     ctx = _lib.Context(local)
     ctx.set_stream(stream.cuda_stream)
     a = s.addr
@@ -577,7 +596,8 @@ def run_multi_rhs(local, stream, steps=3):
     ctx.close()
     for c in cs:
         c.close()
-    return {"workload": f"upwind momentum 64^3 ({s.n} cells), {R} right-hand sides, "
+    return {"workload": f"upwind momentum {dims[0]}x{dims[1]}x{dims[2]} ({s.n} cells), {R} "
+                        "right-hand sides, "
                         "cudaPBiCGStab, tolerance 1e-6",
             "multi_ms": round(ms_m, 3), "sequential_single_ms": round(ms_s, 3),
             "speedup": round(ms_s / ms_m, 3),
@@ -866,6 +886,7 @@ def run_ours(args, ws, rank, local):
             out["batched"] = batched
             out["adjoint"] = run_adjoint(local, stream)
             out["multi_rhs"] = run_multi_rhs(local, stream)
+            out["multi_rhs_128"] = run_multi_rhs(local, stream, steps=2, dims=(128, 128, 128))
             out["configs"], sols = run_small_configs(local, stream)
             psi_gamg, out["gamg"] = run_gamg(ctx, d_diag, d_upper, d_src, stream,
                                              ms_max / args.steps)
