@@ -1,5 +1,5 @@
 """The subdomains' communication over torch.distributed (metal4foam_b200.
-coupled.TorchComm) on world-size-2 gloo process groups on the CPU: the
+coupled.TorchComm) on world-size-2 and -3 gloo process groups on the CPU: the
 callbacks the subdomain solver calls -- the global sum/max and the halo
 exchange -- driven with host buffers, and an FP64 matrix-vector product of
 a decomposed system assembled from them (each rank: its internal product
@@ -68,28 +68,33 @@ def _worker(rank, world, port, out_path):
         ref = O.amul(s, x)[me.cells]
         res["exchange_rc"] = rc
         res["amul_err"] = float(np.max(np.abs(y - ref)) / np.max(np.abs(ref)))
-        # FP32 halo too (the Krylov vectors)
+        # FP32 halo too (the Krylov vectors), from every neighbour
         s32 = [a.astype(np.float32) for a in send]
         r32 = [np.empty(len(i.faceCells), np.float32) for i in me.interfaces]
         sp = (C.c_void_p * len(s32))(*[a.ctypes.data for a in s32])
         rp = (C.c_void_p * len(r32))(*[a.ctypes.data for a in r32])
         rc = cb.exchange(None, len(nb), nb.ctypes.data, nfc.ctypes.data, 4, sp, rp, None)
-        other = subs[1 - rank]
-        back = next(i for i in other.interfaces if i.neighbour == rank)
-        expect = x[other.cells][back.faceCells].astype(np.float32)
-        res["exchange32_ok"] = bool(rc == 0 and np.array_equal(r32[0], expect))
+        ok = rc == 0 and len(me.interfaces) == world - 1
+        for itf, got in zip(me.interfaces, r32):
+            other = subs[itf.neighbour]
+            back = next(i for i in other.interfaces if i.neighbour == rank)
+            ok = ok and np.array_equal(got, x[other.cells][back.faceCells].astype(np.float32))
+        res["exchange32_ok"] = bool(ok)
     finally:
         dist.destroy_process_group()
     with open(out_path + f".{rank}", "w") as f:
         json.dump(res, f)
 
 
-def test_torch_comm_two_gloo_ranks(tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_torch_comm_gloo_ranks(tmp_path, world):
+    """2 ranks (one interface each) and 3 ranks (a random split: every rank
+    has an interface with each of the two others)."""
     import torch.multiprocessing as mp
     out = str(tmp_path / "res")
     ctx = mp.get_context("spawn")
     port = free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, out)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
@@ -99,10 +104,12 @@ def test_torch_comm_two_gloo_ranks(tmp_path):
             p.kill()
             pytest.fail("a rank did not finish")
         assert p.exitcode == 0
-    res = [json.load(open(out + f".{r}")) for r in range(2)]
+    res = [json.load(open(out + f".{r}")) for r in range(world)]
     for r in res:
-        assert r["sum"] == [0, 1.5 + 2.5, 0.0 - 2.0, 1.0 + 10.0]
-        assert r["max"] == [0, 1.25, 0.0]
+        assert r["sum"] == [0, sum(1.5 + k for k in range(world)),
+                            sum(-2.0 * k for k in range(world)),
+                            sum(10.0 ** k for k in range(world))]
+        assert r["max"] == [0, world - 1 + 0.25, 0.0]
         assert r["exchange_rc"] == 0
         assert r["amul_err"] < 1e-13
         assert r["exchange32_ok"]
