@@ -561,12 +561,16 @@ int cf_solve_many_device(cf_context* const* ctx, int32_t count, int32_t solver,
  * neighbouring subdomain.
  *
  * Communication is the caller's (MPI/Pstream, NCCL, or the in-process hub
- * of cf_comm_local_create).  Both callbacks receive device pointers on the
- * subdomain's device and the subdomain's cudaStream_t; they may complete
- * the work before returning or enqueue it on that stream (NCCL), as long as
- * work enqueued on the stream afterwards sees the result.  They return 0 on
- * success.  Every subdomain calls them in the same order with the same
- * counts (all decisions depend on globally reduced values). */
+ * of cf_comm_local_create).  With hostBuffers = 0 both callbacks receive
+ * device pointers on the subdomain's device and the subdomain's
+ * cudaStream_t; they may complete the work before returning or enqueue it
+ * on that stream (NCCL), as long as work enqueued on the stream afterwards
+ * sees the result.  With hostBuffers != 0 they receive host pointers
+ * (pinned staging buffers the library fills before the call and reads back
+ * after it) and must complete the work before returning -- the form for
+ * MPI without CUDA awareness.  They return 0 on success.  Every subdomain
+ * calls them in the same order with the same counts (all decisions depend
+ * on globally reduced values). */
 typedef struct cf_comm
 {
     void* user;
@@ -581,6 +585,8 @@ typedef struct cf_comm
     /* optional: called when this subdomain's solve fails, so the others
      * stop waiting for it */
     void (*abort)(void* user);
+    /* != 0: the callbacks get host buffers (see above); 0: device buffers */
+    int32_t hostBuffers;
 } cf_comm;
 
 typedef struct cf_subdomain cf_subdomain;

@@ -118,7 +118,7 @@ ABORT_FN = C.CFUNCTYPE(None, vp)
 class Comm(C.Structure):
     """cf_comm: the subdomains' communication callbacks."""
     _fields_ = [("user", vp), ("allreduce", ALLREDUCE_FN), ("exchange", EXCHANGE_FN),
-                ("abort", ABORT_FN)]
+                ("abort", ABORT_FN), ("hostBuffers", C.c_int32)]
 
 
 CF_LAYOUT_SELL32 = 0

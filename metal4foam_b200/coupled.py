@@ -49,8 +49,9 @@ def _view(ptr, count, elem_bytes, on_device, torch):
 
 class TorchComm:
     """cf_comm over a torch.distributed process group: every rank is one
-    subdomain, subdomain numbers are group ranks.  `on_device` says whether
-    the solver hands device pointers (NCCL) or host pointers (gloo)."""
+    subdomain, subdomain numbers are group ranks.  `on_device`: the solver
+    hands device buffers (NCCL); otherwise host buffers (gloo, or any
+    backend without device support: the library stages the copies)."""
 
     def __init__(self, group=None, on_device: bool = True):
         import torch
@@ -63,7 +64,8 @@ class TorchComm:
         self._cb_allreduce = _lib.ALLREDUCE_FN(self._allreduce)
         self._cb_exchange = _lib.EXCHANGE_FN(self._exchange)
         self._cb_abort = _lib.ABORT_FN(self._abort)
-        self.comm = _lib.Comm(None, self._cb_allreduce, self._cb_exchange, self._cb_abort)
+        self.comm = _lib.Comm(None, self._cb_allreduce, self._cb_exchange, self._cb_abort,
+                              0 if on_device else 1)
 
     def _allreduce(self, user, values, count, op, stream):
         try:

@@ -123,6 +123,8 @@ struct cf_subdomain
     float* d_D = nullptr;            // [3 n]
     float* d_send32 = nullptr;       // [nH]
     double* d_send64 = nullptr;      // [nH]
+    double* h_send = nullptr;        // [nH] pinned staging of host-buffer communication
+    double* h_recv = nullptr;        // [nH]
     double* d_part = nullptr;
     InnerState* d_st = nullptr;
     DriverState* d_drv = nullptr;
@@ -152,6 +154,9 @@ void free_topology(cf_subdomain* d)
 {
     for (void* p : d->allocs) cudaFree(p);
     d->allocs.clear();
+    if (d->h_send) cudaFreeHost(d->h_send);
+    if (d->h_recv) cudaFreeHost(d->h_recv);
+    d->h_send = d->h_recv = nullptr;
     d->hasTopo = d->hasCoeffs = false;
 }
 
@@ -776,8 +781,20 @@ struct Ctx
 // global sums of `count` per-subdomain values at d_sums (in place)
 int allreduce(Ctx& x, int count, int op)
 {
-    const int rc = x.comm->allreduce(x.comm->user, x.d->d_sums, count, op, (void*)x.d->stream);
+    cf_subdomain* d = x.d;
+    double* buf = d->d_sums;
+    if (x.comm->hostBuffers)
+    {
+        CF_CUDA(cudaMemcpyAsync(d->h_sums, d->d_sums, sizeof(double) * count,
+                                cudaMemcpyDeviceToHost, d->stream));
+        CF_CUDA(cudaStreamSynchronize(d->stream));
+        buf = d->h_sums;
+    }
+    const int rc = x.comm->allreduce(x.comm->user, buf, count, op, (void*)d->stream);
     if (rc != 0) return fail(CF_ERR_CUDA, "cf_comm.allreduce failed (" + std::to_string(rc) + ")");
+    if (x.comm->hostBuffers)
+        CF_CUDA(cudaMemcpyAsync(d->d_sums, d->h_sums, sizeof(double) * count,
+                                cudaMemcpyHostToDevice, d->stream));
     return CF_OK;
 }
 
@@ -791,16 +808,27 @@ int exchange(Ctx& x, T* vec)
     kc_gather_send<T><<<std::max(1, std::min((d->nH + NT - 1) / NT, d->numSMs * 4)), NT, 0,
                         d->stream>>>(d->nH, d->d_sendRow, vec, send);
     CF_LAUNCH();
+    const bool host = x.comm->hostBuffers != 0;
+    T* hs = reinterpret_cast<T*>(d->h_send);
+    T* hr = reinterpret_cast<T*>(d->h_recv);
+    if (host)
+    {
+        CF_CUDA(cudaMemcpyAsync(hs, send, sizeof(T) * d->nH, cudaMemcpyDeviceToHost, d->stream));
+        CF_CUDA(cudaStreamSynchronize(d->stream));
+    }
     std::vector<const void*> s(d->nIf);
     std::vector<void*> r(d->nIf);
     for (int p = 0; p < d->nIf; ++p)
     {
-        s[p] = send + d->haloOff[p];
-        r[p] = vec + d->n + d->haloOff[p];
+        s[p] = host ? (const void*)(hs + d->haloOff[p]) : (const void*)(send + d->haloOff[p]);
+        r[p] = host ? (void*)(hr + d->haloOff[p]) : (void*)(vec + d->n + d->haloOff[p]);
     }
     const int rc = x.comm->exchange(x.comm->user, d->nIf, d->nbr.data(), d->nFaces.data(),
                                     (int32_t)sizeof(T), s.data(), r.data(), (void*)d->stream);
     if (rc != 0) return fail(CF_ERR_CUDA, "cf_comm.exchange failed (" + std::to_string(rc) + ")");
+    if (host)
+        CF_CUDA(cudaMemcpyAsync(vec + d->n, hr, sizeof(T) * d->nH, cudaMemcpyHostToDevice,
+                                d->stream));
     return CF_OK;
 }
 
@@ -1369,6 +1397,8 @@ extern "C" int cf_subdomain_set_topology(cf_subdomain* d, int32_t n, int32_t nf,
     CF_TRY(sd_alloc(d, &d->d_D, 3 * N));
     CF_TRY(sd_alloc(d, &d->d_send32, (size_t)std::max(nH, 1LL)));
     CF_TRY(sd_alloc(d, &d->d_send64, (size_t)std::max(nH, 1LL)));
+    CF_CUDA(cudaMallocHost((void**)&d->h_send, sizeof(double) * (size_t)std::max(nH, 1LL)));
+    CF_CUDA(cudaMallocHost((void**)&d->h_recv, sizeof(double) * (size_t)std::max(nH, 1LL)));
     cudaStream_t s = d->stream;
     CF_CUDA(cudaMemcpyAsync(d->d_sliceOff, L.sliceOff.data(), sizeof(int32_t) * L.sliceOff.size(),
                             cudaMemcpyHostToDevice, s));
@@ -1620,6 +1650,7 @@ extern "C" int cf_comm_local_create(int32_t nRanks, double timeoutSeconds, cf_co
         comms[r].allreduce = local_allreduce;
         comms[r].exchange = local_exchange;
         comms[r].abort = local_abort;
+        comms[r].hostBuffers = 0;
     }
     return CF_OK;
 }

@@ -174,3 +174,91 @@ def test_mismatched_interface_fails_every_subdomain(require_gpu):
     for sv in solvers:
         sv.close()
     comm.close()
+
+
+class _HostThreadsComm:
+    """cf_comm with host buffers (hostBuffers = 1), written in Python for
+    the subdomains of one process: the form an MPI (Pstream) caller
+    without CUDA awareness uses.  Sums fold in rank order, as the
+    in-process hub's do."""
+
+    def __init__(self, k, subs):
+        import ctypes as C
+        self.k = k
+        self.bar = threading.Barrier(k, timeout=60)
+        self.vals = [None] * k
+        self.sends = [None] * k
+        self.comms = []
+        for r in range(k):
+            def allreduce(user, values, count, op, stream, r=r):
+                try:
+                    v = np.ctypeslib.as_array((C.c_double * count).from_address(values))
+                    self.vals[r] = v.copy()
+                    self.bar.wait()
+                    out = self.vals[0].copy()
+                    for q in range(1, k):
+                        out = np.maximum(out, self.vals[q]) if op == 1 else out + self.vals[q]
+                    self.bar.wait()
+                    v[:] = out
+                    return 0
+                except Exception:  # noqa: BLE001
+                    return 1
+
+            def exchange(user, nif, nb, nfc, eb, send, recv, stream, r=r):
+                try:
+                    ct = C.c_double if eb == 8 else C.c_float
+                    nbs = np.ctypeslib.as_array((C.c_int32 * nif).from_address(nb))
+                    nfs = np.ctypeslib.as_array((C.c_int32 * nif).from_address(nfc))
+                    sp = (C.c_void_p * nif).from_address(send)
+                    rp = (C.c_void_p * nif).from_address(recv)
+                    self.sends[r] = {int(nbs[p]): np.ctypeslib.as_array(
+                        (ct * int(nfs[p])).from_address(sp[p])).copy() for p in range(nif)}
+                    self.bar.wait()
+                    for p in range(nif):
+                        got = self.sends[int(nbs[p])][r]
+                        np.ctypeslib.as_array((ct * int(nfs[p])).from_address(rp[p]))[:] = got
+                    self.bar.wait()
+                    return 0
+                except Exception:  # noqa: BLE001
+                    return 1
+
+            cbs = (_lib.ALLREDUCE_FN(allreduce), _lib.EXCHANGE_FN(exchange),
+                   _lib.ABORT_FN(lambda user: self.bar.abort()))
+            self.comms.append((_lib.Comm(None, cbs[0], cbs[1], cbs[2], 1), cbs))
+
+    def __getitem__(self, r):
+        return self.comms[r][0]
+
+
+def test_host_buffer_communication_equals_device(require_gpu):
+    """The same decomposed solve with the in-process hub (device buffers)
+    and with a host-buffer communicator: bit-identical results."""
+    s = mesh.varcoeff3d((28, 26, 24), seed=13)
+    part = decompose.slab_partition(s.n, 2)
+    subs, psis_dev, perfs_dev, errs = solve_decomposed(s, part, 2, _lib.CF_SOLVER_PCG)
+    assert errs == [None, None]
+    solvers = [_lib.SubdomainSolver(sd) for sd in subs]
+    comm = _HostThreadsComm(2, subs)
+    opts = _lib.default_options()
+    psis = [np.zeros(sd.n) for sd in subs]
+    perfs, errs = [None, None], [None, None]
+
+    def run(r):
+        try:
+            perfs[r] = solvers[r].solve(_lib.CF_SOLVER_PCG, psis[r], subs[r].system.source, opts,
+                                        comm[r])
+        except Exception as e:  # noqa: BLE001
+            errs[r] = e
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(600)
+    assert errs == [None, None], errs
+    for r in range(2):
+        assert np.array_equal(psis[r], psis_dev[r])
+        assert perfs[r].nIterations == perfs_dev[r].nIterations
+        assert perfs[r].finalResidual == perfs_dev[r].finalResidual
+    for sv in solvers:
+        sv.close()
