@@ -9,6 +9,8 @@
 
 #include "cudaFoamSolver.H"
 #include "PrecisionAdaptor.H"
+#include "Pstream.H"
+#include "processorLduInterface.H"
 #include "cudafoam.h"
 
 #include <fenv.h>
@@ -17,6 +19,7 @@
 #include <set>
 #include <sstream>
 #include <string>
+#include <vector>
 
 static_assert
 (
@@ -45,6 +48,62 @@ struct FpTrapGuard
 struct ContextDeleter
 {
     void operator()(cf_context* c) const { cf_context_destroy(c); }
+};
+
+struct SubdomainDeleter
+{
+    void operator()(cf_subdomain* d) const { cf_subdomain_destroy(d); }
+};
+
+// The subdomain solve's communication over Pstream (MPI): global sums and
+// maxima by reduce, halo values by non-blocking raw transfers with each
+// neighbouring processor.  The library stages device data through host
+// buffers (hostBuffers = 1), so MPI needs no CUDA awareness.
+struct PstreamComm
+{
+    Foam::label comm;
+    int tag;
+
+    static int allreduce(void* user, double* values, int32_t count, int32_t op, void*)
+    {
+        const PstreamComm& c = *static_cast<const PstreamComm*>(user);
+        for (int32_t i = 0; i < count; ++i)
+        {
+            if (op == 1)
+                Foam::reduce(values[i], Foam::maxOp<double>(), c.tag, c.comm);
+            else
+                Foam::reduce(values[i], Foam::sumOp<double>(), c.tag, c.comm);
+        }
+        return 0;
+    }
+
+    static int exchange(void* user, int32_t nInterfaces, const int32_t* neighbour,
+                        const int32_t* nFaces, int32_t elemBytes, const void* const* send,
+                        void* const* recv, void*)
+    {
+        const PstreamComm& c = *static_cast<const PstreamComm*>(user);
+        const Foam::label start = Foam::UPstream::nRequests();
+        for (int32_t p = 0; p < nInterfaces; ++p)
+        {
+            Foam::UIPstream::read
+            (
+                Foam::UPstream::commsTypes::nonBlocking, neighbour[p],
+                static_cast<char*>(recv[p]), std::streamsize(nFaces[p])*elemBytes, c.tag,
+                c.comm
+            );
+        }
+        for (int32_t p = 0; p < nInterfaces; ++p)
+        {
+            Foam::UOPstream::write
+            (
+                Foam::UPstream::commsTypes::nonBlocking, neighbour[p],
+                static_cast<const char*>(send[p]), std::streamsize(nFaces[p])*elemBytes,
+                c.tag, c.comm
+            );
+        }
+        Foam::UPstream::waitRequests(start);
+        return 0;
+    }
 };
 
 int deflateMode(const Foam::word& w)
@@ -133,18 +192,32 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     const direction cmpt
 ) const
 {
-    // Coupled interfaces (processor/cyclic/AMI) cannot be applied inside the
-    // device-resident iteration.
+    // Processor interfaces of a decomposed case: the subdomain solve
+    // (halo exchange and global sums over Pstream).  Other coupled
+    // interfaces (cyclic/AMI) cannot be applied inside the device-resident
+    // iteration, as in the reference (metalFoamSolver.C:89-99).
+    bool decomposed = false;
     forAll(interfaces_, patchi)
     {
         if (interfaces_.set(patchi))
         {
-            FatalErrorInFunction
-                << solverName << " does not support coupled boundaries "
-                << "(processor/cyclic/AMI); run serially on a mesh "
-                << "without coupled patches."
-                << exit(FatalError);
+            if
+            (
+                !UPstream::parRun()
+             || !isA<processorLduInterface>(interfaces_[patchi].interface())
+            )
+            {
+                FatalErrorInFunction
+                    << solverName << " supports processor interfaces only "
+                    << "(no cyclic/AMI coupled boundaries)."
+                    << exit(FatalError);
+            }
+            decomposed = true;
         }
+    }
+    if (decomposed)
+    {
+        return solveDecomposed(solverName, useBiCGStab, psi, source);
     }
 
     (void)cmpt;   // every component of a segregated solve is a scalar system here
@@ -193,30 +266,7 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
         "cf_set_coeffs"
     );
 
-    cf_options opts;
-    cf_options_default(&opts);
-    opts.tolerance = tolerance_;
-    opts.relTol = relTol_;
-    opts.maxIter = maxIter_;
-    opts.minIter = minIter_;
-    opts.maxRestarts = cudaDict_.getOrDefault<label>("maxRestarts", 8);
-    opts.iterationsPerSync = cudaDict_.getOrDefault<label>("iterationsPerSync", 1);
-    opts.deflate = deflateMode(cudaDict_.getOrDefault<word>("deflate", "auto"));
-    opts.chebyshevOrder = cudaDict_.getOrDefault<label>("chebyshevOrder", 8);
-    opts.chebyshevRatio = cudaDict_.getOrDefault<scalar>("chebyshevRatio", 30.0);
-    opts.profile = cudaDict_.getOrDefault<bool>("profile", false);
-    opts.verbose = cudaDict_.getOrDefault<bool>("verbose", false);
-    opts.graph = cudaDict_.getOrDefault<bool>("graph", true);
-    opts.stagnationLimit = cudaDict_.getOrDefault<label>("stagnationLimit", 0);
-    opts.persistentMaxCells = cudaDict_.getOrDefault<label>("persistentMaxCells", 0);
-    opts.clusterMaxCells = cudaDict_.getOrDefault<label>("clusterMaxCells", 0);
-    opts.preconditioner =
-        preconditionerKind(cudaDict_.getOrDefault<word>("preconditioner", "Chebyshev"));
-    opts.nSweeps = cudaDict_.getOrDefault<label>("nSweeps", 3);
-    opts.nCellsInCoarsestLevel = cudaDict_.getOrDefault<label>("nCellsInCoarsestLevel", 128);
-    opts.scaleCorrection = cudaDict_.getOrDefault<scalar>("scaleCorrection", 1.8);
-    opts.smootherRatio = cudaDict_.getOrDefault<scalar>("smootherRatio", 8.0);
-
+    cf_options opts = cudaOptions();
     // autotune yes: time the SpMV launch shapes once per context (the mesh
     // of a context does not change during a run) and keep the fastest
     if (cudaDict_.getOrDefault<bool>("autotune", false))
@@ -276,6 +326,145 @@ Foam::solverPerformance Foam::cudaFoamSolver::solveImpl
     {
         Info<< "    " << solverName << " profile: tConvert=" << 1000*tConvert
             << "ms" << nl;
+    }
+    return solverPerf;
+}
+
+cf_options Foam::cudaFoamSolver::cudaOptions() const
+{
+    cf_options opts;
+    cf_options_default(&opts);
+    opts.tolerance = tolerance_;
+    opts.relTol = relTol_;
+    opts.maxIter = maxIter_;
+    opts.minIter = minIter_;
+    opts.maxRestarts = cudaDict_.getOrDefault<label>("maxRestarts", 8);
+    opts.iterationsPerSync = cudaDict_.getOrDefault<label>("iterationsPerSync", 1);
+    opts.deflate = deflateMode(cudaDict_.getOrDefault<word>("deflate", "auto"));
+    opts.chebyshevOrder = cudaDict_.getOrDefault<label>("chebyshevOrder", 8);
+    opts.chebyshevRatio = cudaDict_.getOrDefault<scalar>("chebyshevRatio", 30.0);
+    opts.profile = cudaDict_.getOrDefault<bool>("profile", false);
+    opts.verbose = cudaDict_.getOrDefault<bool>("verbose", false);
+    opts.graph = cudaDict_.getOrDefault<bool>("graph", true);
+    opts.stagnationLimit = cudaDict_.getOrDefault<label>("stagnationLimit", 0);
+    opts.persistentMaxCells = cudaDict_.getOrDefault<label>("persistentMaxCells", 0);
+    opts.clusterMaxCells = cudaDict_.getOrDefault<label>("clusterMaxCells", 0);
+    opts.preconditioner =
+        preconditionerKind(cudaDict_.getOrDefault<word>("preconditioner", "Chebyshev"));
+    opts.nSweeps = cudaDict_.getOrDefault<label>("nSweeps", 3);
+    opts.nCellsInCoarsestLevel = cudaDict_.getOrDefault<label>("nCellsInCoarsestLevel", 128);
+    opts.scaleCorrection = cudaDict_.getOrDefault<scalar>("scaleCorrection", 1.8);
+    opts.smootherRatio = cudaDict_.getOrDefault<scalar>("smootherRatio", 8.0);
+
+    return opts;
+}
+
+
+Foam::solverPerformance Foam::cudaFoamSolver::solveDecomposed
+(
+    const word& solverName,
+    const bool useBiCGStab,
+    solveScalarField& psi,
+    const solveScalarField& source
+) const
+{
+    FpTrapGuard fpe;
+    auto check = [&](int rc, const char* what)
+    {
+        if (rc != CF_OK)
+        {
+            FatalErrorInFunction
+                << solverName << ": " << what << " failed: " << cf_last_error()
+                << exit(FatalError);
+        }
+    };
+
+    // processor patches in patch order: neighbour, faceCells, coefficients
+    std::vector<int32_t> neighbour, nIfFaces, faceCells;
+    std::vector<double> ifCoeffs;
+    label comm = UPstream::worldComm;
+    int tag = UPstream::msgType();
+    forAll(interfaces_, patchi)
+    {
+        if (!interfaces_.set(patchi)) continue;
+        const lduInterface& iface = interfaces_[patchi].interface();
+        const processorLduInterface& proc = refCast<processorLduInterface>(iface);
+        const labelUList& fc = iface.faceCells();
+        const Field<scalar>& coeffs = interfaceBouCoeffs_[patchi];
+        neighbour.push_back(proc.neighbProcNo());
+        nIfFaces.push_back(fc.size());
+        for (label k = 0; k < fc.size(); ++k)
+        {
+            faceCells.push_back(fc.cdata()[k]);
+            ifCoeffs.push_back(coeffs.cdata()[k]);
+        }
+        comm = proc.comm();
+        tag = proc.tag();
+    }
+
+    // one subdomain per (field, mesh) for the run; topology set once
+    static std::map<std::string, std::unique_ptr<cf_subdomain, SubdomainDeleter>> cache;
+    std::ostringstream key;
+    key << fieldName_ << '@' << static_cast<const void*>(&matrix_.mesh());
+    auto& slot = cache[key.str()];
+    const lduAddressing& addr = matrix_.mesh().lduAddr();
+    if (!slot)
+    {
+        cf_subdomain* d = nullptr;
+        check(cf_subdomain_create(&d, 0), "cf_subdomain_create");
+        slot.reset(d);
+        check
+        (
+            cf_subdomain_set_topology
+            (
+                d, addr.size(), addr.upperAddr().size(),
+                addr.lowerAddr().cdata(), addr.upperAddr().cdata(),
+                addr.ownerStartAddr().cdata(), addr.losortAddr().cdata(),
+                addr.losortStartAddr().cdata(),
+                int32_t(neighbour.size()), neighbour.data(), nIfFaces.data(),
+                faceCells.data(), CF_REORDER_AUTO
+            ),
+            "cf_subdomain_set_topology"
+        );
+    }
+    check
+    (
+        cf_subdomain_set_coeffs
+        (
+            slot.get(), matrix_.diag().cdata(), matrix_.upper().cdata(),
+            matrix_.hasLower() ? matrix_.lower().cdata() : nullptr, ifCoeffs.data()
+        ),
+        "cf_subdomain_set_coeffs"
+    );
+
+    PstreamComm pc{comm, tag};
+    cf_comm cc;
+    cc.user = &pc;
+    cc.allreduce = &PstreamComm::allreduce;
+    cc.exchange = &PstreamComm::exchange;
+    cc.abort = nullptr;
+    cc.hostBuffers = 1;
+
+    const cf_options opts = cudaOptions();
+    cf_performance perf;
+    check
+    (
+        cf_subdomain_solve
+        (
+            slot.get(), useBiCGStab ? CF_SOLVER_PBICGSTAB : CF_SOLVER_PCG, psi.data(),
+            source.cdata(), &opts, &cc, &perf
+        ),
+        "cf_subdomain_solve"
+    );
+
+    solverPerformance solverPerf(solverName, fieldName_);
+    solverPerf.initialResidual() = perf.initialResidual;
+    solverPerf.finalResidual() = perf.finalResidual;
+    solverPerf.nIterations() = perf.nIterations;
+    solverPerf.checkConvergence(tolerance_, relTol_, log_);
+    if (perf.singular)
+    {
+        solverPerf.checkSingularity(0);
     }
     return solverPerf;
 }

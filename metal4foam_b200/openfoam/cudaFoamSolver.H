@@ -50,6 +50,7 @@ SourceFiles
 #include "lduMatrix.H"
 
 struct cf_context;
+#include "cudafoam.h"
 
 namespace Foam
 {
@@ -65,6 +66,19 @@ protected:
 
         //- The device context of this (field, mesh); created on first use
         cf_context* backend() const;
+
+        //- The solver controls as the C ABI takes them
+        cf_options cudaOptions() const;
+
+        //- Decomposed case: this processor's subdomain, processor
+        //  interfaces coupled over Pstream (cf_subdomain_solve)
+        solverPerformance solveDecomposed
+        (
+            const word& solverName,
+            const bool useBiCGStab,
+            solveScalarField& psi,
+            const solveScalarField& source
+        ) const;
 
         //- The FP64 driver + GPU solve
         solverPerformance solveImpl

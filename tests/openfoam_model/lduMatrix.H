@@ -53,16 +53,43 @@ typedef Field<solveScalar> solveScalarField;
 template <template <class> class F, class T>
 class FieldField
 {
+public:
+    const F<T>& operator[](label i) const;
 };
 
-class lduInterfaceField;
+class lduInterface
+{
+public:
+    virtual ~lduInterface() = default;
+    virtual const labelUList& faceCells() const = 0;
+};
+
+class lduInterfaceField
+{
+public:
+    virtual ~lduInterfaceField() = default;
+    const lduInterface& interface() const;
+};
 
 class lduInterfaceFieldPtrsList
 {
 public:
     label size() const;
     bool set(label i) const;
+    const lduInterfaceField& operator[](label i) const;
 };
+
+template <class Type, class U>
+inline bool isA(const U& t)
+{
+    return dynamic_cast<const Type*>(&t) != nullptr;
+}
+
+template <class Type, class U>
+inline const Type& refCast(const U& t)
+{
+    return dynamic_cast<const Type&>(t);
+}
 
 class dictionary
 {

@@ -2,7 +2,9 @@
 (no OpenFOAM); it is compiled with -fsyntax-only against the C ABI header
 and a minimal model of the OpenFOAM interfaces it uses
 (tests/openfoam_model/), so its calls into include/cudafoam.h are
-type-checked and every control key the Python surface accepts is read."""
+type-checked and every control key the Python surface accepts is read.
+The model includes the processor-interface and Pstream calls the adapter
+makes for decomposed cases (cf_subdomain_* with a Pstream cf_comm)."""
 import glob
 import os
 import re
@@ -32,3 +34,11 @@ def test_adapter_reads_every_control_key():
     text = open(os.path.join(ADAPTER, "cudaFoamSolver.C")).read()
     read = set(re.findall(r'getOrDefault<[^>]+>\("([A-Za-z]+)"', text))
     assert set(_CONTROL_KEYS) <= read, sorted(set(_CONTROL_KEYS) - read)
+
+
+def test_adapter_routes_processor_interfaces_to_subdomains():
+    text = open(os.path.join(ADAPTER, "cudaFoamSolver.C")).read()
+    for call in ("cf_subdomain_set_topology", "cf_subdomain_set_coeffs", "cf_subdomain_solve",
+                 "isA<processorLduInterface>", "interfaceBouCoeffs_[patchi]",
+                 "hostBuffers = 1"):
+        assert call in text, call
