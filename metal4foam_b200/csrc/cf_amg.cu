@@ -932,8 +932,16 @@ int amg_stage(cf_context* c, int deflate, float scaleCorrection)
     }
     AmgLevel& Z = d->lv.back();
     const int smem = (Z.n * Z.n + Z.n) * (int)sizeof(double);
+    // the attribute is the function's, shared by every context of the
+    // process: always the same value (the largest coarsest level, 128
+    // cells), so concurrent solves on other threads never lower it under a
+    // launch that needs more
+    constexpr int kMaxCoarse = 128;
+    static_assert((kMaxCoarse * kMaxCoarse + kMaxCoarse) * sizeof(double) <= 227 * 1024,
+                  "coarsest inverse must fit one CTA's shared memory");
+    if (Z.n > kMaxCoarse) return fail(CF_ERR_UNSUPPORTED, "GAMG coarsest level above 128 cells");
     AMG_CUDA(cudaFuncSetAttribute(ka_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  smem));
+                                  (kMaxCoarse * kMaxCoarse + kMaxCoarse) * (int)sizeof(double)));
     ka_coarse_invert<<<1, AMG_INV_THREADS, smem, s>>>(Z.n, Z.A.sliceOff, Z.A.col, Z.eface,
                                                       Z.upper64, Z.diag64, deflate ? 1 : 0,
                                                       d->coarseInv);

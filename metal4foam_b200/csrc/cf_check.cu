@@ -267,7 +267,9 @@ extern "C" int cf_inner_step(cf_context* c, int32_t step, cf_step_io* io)
     io->sums[0] = io->sums[1] = io->sums[2] = 0.0;
     switch (step)
     {
-        case CF_STEP_CHEB: io->sums[0] = st.wArA; break;   // z.r (last step only)
+        case CF_STEP_CHEB:   // z.r, formed by the last step only
+            io->sums[0] = io->chebStep == io->chebOrder - 1 ? st.wArA : 0.0;
+            break;
         case CF_STEP_PCG_P_SPMV: io->sums[0] = st.wApA; break;
         case CF_STEP_PCG_UPDATE:
             io->sums[0] = st.res;                          // sum |rA|

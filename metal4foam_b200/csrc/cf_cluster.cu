@@ -360,8 +360,12 @@ int cluster_inner(cf_context* c, int order, int maxCells, bool* ran)
     const int cs = (n + rpc - 1) / rpc;
     const size_t smem = sizeof(float) * NVEC * (size_t)rpc;
     const void* fn = order > 1 ? (const void*)kc_pcg<true> : (const void*)kc_pcg<false>;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess ||
+    // the attribute is the function's, shared by every context of the
+    // process: always the largest value (one row per thread of a full CTA),
+    // so a concurrent solve on another thread never lowers it under this
+    // launch
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(float) * NVEC * (size_t)CT)) != cudaSuccess ||
         cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
     {
         cudaGetLastError();
