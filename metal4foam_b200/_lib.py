@@ -173,6 +173,7 @@ SIGNATURES = [
     ("cf_batch_kernel_launches", C.c_int, [vp, C.POINTER(C.c_longlong)]),
     ("cf_batch_add_system", C.c_int, [vp, i32, i32, vp, vp, vp, vp, vp, C.POINTER(i32)]),
     ("cf_batch_finalize", C.c_int, [vp, i32]),
+    ("cf_batch_set_solo_cells", C.c_int, [vp, i32]),
     ("cf_batch_set_coeffs", C.c_int, [vp, i32, vp, vp, vp]),
     ("cf_batch_set_coeffs_device", C.c_int, [vp, i32, vp, vp, vp]),
     ("cf_batch_solve", C.c_int, [vp, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(Options),
@@ -549,6 +550,9 @@ class Batch:
                                          *(ptr(a) for a in arrs), C.byref(idx)))
         self.sizes.append((addr.n, addr.nf))
         return idx.value
+
+    def set_solo_cells(self, min_cells):
+        check(load().cf_batch_set_solo_cells(self.h, int(min_cells)))
 
     def finalize(self, reorder="auto"):
         check(load().cf_batch_finalize(self.h, REORDER[reorder]))

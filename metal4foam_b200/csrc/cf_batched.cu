@@ -26,6 +26,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace cf;
@@ -964,6 +965,12 @@ struct cf_batch
     };
     std::vector<Sys> sys;
     int S = 0;
+    // systems that fill the GPU on their own run as single solves (one
+    // context each, own stream) concurrently with the batched rest
+    int32_t soloMinCells = 0;        // 0: automatic, < 0: never
+    std::vector<cf_context*> solo;   // caller's index -> its context, or null
+    std::vector<int> inner;          // caller's index -> index among the batched systems
+    int nAll = 0;                    // systems as the caller numbers them
     long long N = 0, NF = 0, nnzp = 0;
     int nslices = 0, nTiles = 0;
 
@@ -1469,6 +1476,8 @@ extern "C" int cf_batch_destroy(cf_batch* bt)
     if (!bt) return CF_OK;
     cudaSetDevice(bt->device);
     if (bt->stream) cudaStreamSynchronize(bt->stream);
+    for (cf_context* c : bt->solo)
+        if (c) cf_context_destroy(c);
     for (auto& kv : bt->graphs) cudaGraphExecDestroy(kv.second);
     for (void* p : bt->allocs) cudaFree(p);
     if (bt->h_drv) cudaFreeHost(bt->h_drv);
@@ -1491,7 +1500,13 @@ extern "C" int cf_batch_set_stream(cf_batch* bt, void* stream)
 extern "C" int cf_batch_kernel_launches(const cf_batch* bt, long long* count)
 {
     if (!bt || !count) return fail(CF_ERR_INVALID_ARG, "NULL argument");
-    *count = bt->launches;
+    long long n = bt->launches;
+    for (const cf_context* c : bt->solo)
+    {
+        long long k = 0;
+        if (c && cf_context_kernel_launches(c, &k) == CF_OK) n += k;
+    }
+    *count = n;
     return CF_OK;
 }
 
@@ -1524,6 +1539,42 @@ extern "C" int cf_batch_finalize(cf_batch* bt, int32_t reorder)
     if (bt->finalized) return CF_OK;
     if (bt->sys.empty()) return fail(CF_ERR_INVALID_ARG, "batch has no systems");
     CFB_CUDA(cudaSetDevice(bt->device));
+    // systems with at least a full resident grid of rows (every SM busy on
+    // their own) become solo systems
+    {
+        const long long minCells =
+            bt->soloMinCells > 0 ? bt->soloMinCells
+                                 : (bt->soloMinCells == 0
+                                        ? (long long)bt->numSMs * bt->maxBlocksPerSM * NT
+                                        : (1LL << 62));
+        bt->nAll = (int)bt->sys.size();
+        bt->solo.assign(bt->nAll, nullptr);
+        bt->inner.assign(bt->nAll, -1);
+        std::vector<cf_batch::Sys> keep;
+        for (int i = 0; i < bt->nAll; ++i)
+        {
+            auto& y = bt->sys[i];
+            if ((long long)y.n < minCells)
+            {
+                bt->inner[i] = (int)keep.size();
+                keep.push_back(std::move(y));
+                continue;
+            }
+            cf_context* c = nullptr;
+            CFB_TRY(cf_context_create(&c, bt->device));
+            bt->solo[i] = c;
+            CFB_TRY(cf_context_set_reorder(c, reorder));
+            CFB_TRY(cf_set_topology(c, y.n, y.nf, y.low.data(), y.upp.data(), y.own.data(),
+                                    y.los.data(), y.losS.data()));
+        }
+        bt->sys.swap(keep);
+        if (bt->sys.empty())
+        {
+            bt->S = 0;
+            bt->finalized = true;
+            return CF_OK;
+        }
+    }
     bt->S = (int)bt->sys.size();
     long long row = 0, face = 0, ent = 0;
     int tile = 0, slices = 0;
@@ -1680,8 +1731,17 @@ static int batch_set_coeffs(cf_batch* bt, int32_t i, const double* diag, const d
                             const double* lower, cudaMemcpyKind kind)
 {
     if (!bt || !bt->finalized) return fail(CF_ERR_INVALID_ARG, "batch not finalised");
-    if (i < 0 || i >= bt->S) return fail(CF_ERR_INVALID_ARG, "system index out of range");
+    if (i < 0 || i >= bt->nAll) return fail(CF_ERR_INVALID_ARG, "system index out of range");
     if (lower) return fail(CF_ERR_UNSUPPORTED, "batched solves take symmetric matrices (PCG)");
+    if (bt->solo[i])
+    {
+        if (kind == cudaMemcpyHostToDevice)
+            return cf_set_coeffs(bt->solo[i], diag, upper, nullptr, nullptr);
+        // device data: ordered after the batch stream's earlier work
+        CFB_CUDA(cudaStreamSynchronize(bt->stream));
+        return cf_set_coeffs_device(bt->solo[i], diag, upper, nullptr);
+    }
+    i = bt->inner[i];
     const auto& y = bt->sys[i];
     if (!diag || (y.nf > 0 && !upper)) return fail(CF_ERR_INVALID_ARG, "NULL coefficient array");
     CFB_CUDA(cudaSetDevice(bt->device));
@@ -1727,12 +1787,76 @@ static int batch_check(cf_batch* bt, int32_t solver, const cf_options* o, cf_per
     return CF_OK;
 }
 
+// The batched systems through batch_solve on the calling thread, each solo
+// system through cf_solve[_device] on a thread and stream of its own, all at
+// once; every system gets what its own path returns.
+static int batch_solve_all(cf_batch* bt, double* const* psi, const double* const* src,
+                           bool hostPtrs, const cf_options* o, cf_performance* perf)
+{
+    std::vector<double*> ip;
+    std::vector<const double*> is;
+    std::vector<int> solos;
+    for (int i = 0; i < bt->nAll; ++i)
+    {
+        if (bt->solo[i])
+        {
+            solos.push_back(i);
+        }
+        else
+        {
+            ip.push_back(psi[i]);
+            is.push_back(src[i]);
+        }
+    }
+    if (!solos.empty() && !hostPtrs) CFB_CUDA(cudaStreamSynchronize(bt->stream));
+    std::vector<int> rc(bt->nAll, CF_OK);
+    std::vector<std::string> msg(bt->nAll);
+    auto run = [&](int i) {
+        const int r = hostPtrs ? cf_solve(bt->solo[i], CF_SOLVER_PCG, psi[i], src[i], o, &perf[i])
+                               : cf_solve_device(bt->solo[i], CF_SOLVER_PCG, psi[i], src[i], o,
+                                                 &perf[i]);
+        if (r != CF_OK) msg[i] = cf_last_error();
+        rc[i] = r;
+    };
+    std::vector<std::thread> pool;
+    std::vector<int> inlineRuns;
+    for (int i : solos)
+    {
+        try
+        {
+            pool.emplace_back(run, i);
+        }
+        catch (...)
+        {
+            inlineRuns.push_back(i);   // no exception crosses the C ABI
+        }
+    }
+    int brc = CF_OK;
+    std::string bmsg;
+    if (bt->S > 0)
+    {
+        std::vector<cf_performance> bp(bt->S);
+        brc = batch_solve(bt, ip.data(), is.data(), hostPtrs, o, bp.data());
+        if (brc != CF_OK)
+            bmsg = cf_last_error();
+        else
+            for (int i = 0; i < bt->nAll; ++i)
+                if (!bt->solo[i]) perf[i] = bp[bt->inner[i]];
+    }
+    for (int i : inlineRuns) run(i);
+    for (auto& t : pool) t.join();
+    if (brc != CF_OK) return fail(brc, bmsg);
+    for (int i : solos)
+        if (rc[i] != CF_OK) return fail(rc[i], "system " + std::to_string(i) + ": " + msg[i]);
+    return CF_OK;
+}
+
 extern "C" int cf_batch_solve(cf_batch* bt, int32_t solver, double* const* psi,
                               const double* const* source, const cf_options* o,
                               cf_performance* perf)
 {
     CFB_TRY(batch_check(bt, solver, o, perf, psi, source));
-    return batch_solve(bt, psi, source, true, o, perf);
+    return batch_solve_all(bt, psi, source, true, o, perf);
 }
 
 extern "C" int cf_batch_solve_device(cf_batch* bt, int32_t solver, double* const* psi,
@@ -1740,5 +1864,13 @@ extern "C" int cf_batch_solve_device(cf_batch* bt, int32_t solver, double* const
                                      cf_performance* perf)
 {
     CFB_TRY(batch_check(bt, solver, o, perf, psi, source));
-    return batch_solve(bt, psi, source, false, o, perf);
+    return batch_solve_all(bt, psi, source, false, o, perf);
+}
+
+extern "C" int cf_batch_set_solo_cells(cf_batch* bt, int32_t minCells)
+{
+    if (!bt) return fail(CF_ERR_INVALID_ARG, "batch is NULL");
+    if (bt->finalized) return fail(CF_ERR_INVALID_ARG, "batch already finalised");
+    bt->soloMinCells = minCells;
+    return CF_OK;
 }

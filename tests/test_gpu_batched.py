@@ -165,3 +165,36 @@ def test_batch_one_persistent_launch_bitwise(require_gpu, order):
             assert getattr(p, f) == getattr(q, f), f
     assert lb <= la, (lb, la)     # one launch per restart instead of one graph launch
     bt.close()
+
+
+def test_batch_solo_systems(require_gpu):
+    """Systems above the solo size run as single solves on their own
+    threads and streams, concurrently with the batched launches of the
+    rest: a solo system's result is bit for bit its cf_solve result, the
+    batched ones behave as in the plain batch."""
+    systems = small_systems()
+    opts = _lib.default_options(maxRestarts=8, maxIter=3000)
+    src = [s.source for s in systems]
+    bt = _lib.Batch(0)
+    for s in systems:
+        bt.add_system(s.addr)
+    bt.set_solo_cells(5000)
+    bt.finalize()
+    for i, s in enumerate(systems):
+        bt.set_coeffs(i, s.diag, s.upper)
+    psis = [np.zeros(s.n) for s in systems]
+    perfs = bt.solve(psis, src, opts)
+    ref = make_batch(systems)
+    rpsis = [np.zeros(s.n) for s in systems]
+    rperfs = ref.solve(rpsis, src, opts)
+    for s, psi, p, rp, rpsi in zip(systems, psis, perfs, rperfs, rpsis):
+        if s.n >= 5000:
+            x1, p1 = single_solve(s, opts)
+            assert np.array_equal(psi, x1), s.name
+            assert p.nIterations == p1.nIterations and p.finalResidual == p1.finalResidual
+        else:
+            assert np.array_equal(psi, rpsi), s.name
+            assert p.nIterations == rp.nIterations
+        assert p.converged and p.finalResidual < 1e-6
+    bt.close()
+    ref.close()
