@@ -285,24 +285,33 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
     du = [torch.from_numpy(s.upper).to(dev) for s in loc]
     db = [torch.from_numpy(s.source).to(dev) for s in loc]
     dp = [torch.zeros(s.n, dtype=torch.float64, device=dev) for s in loc]
-    bt = None
+    # bt: the batch as the library runs it by default (systems that fill the
+    # GPU alone as single solves on their own streams, the rest batched);
+    # bt_one: every system in the one-launch-per-phase batch
+    bt = bt_one = None
     if loc:
         bt = _lib.Batch(local)
-        bt.set_stream(stream.cuda_stream)
-        for s in loc:
-            bt.add_system(s.addr)
-        bt.finalize()
+        bt_one = _lib.Batch(local)
+        for b, solo in ((bt, 0), (bt_one, -1)):
+            b.set_stream(stream.cuda_stream)
+            for s in loc:
+                b.add_system(s.addr)
+            b.set_solo_cells(solo)
+            b.finalize()
     o = _lib.default_options(**opts)
     res = {"b": [], "p": []}
+    cur = {"bt": bt}
+    solo_min = torch.cuda.get_device_properties(dev).multi_processor_count * 2048
 
     def batched():
-        if bt is None:
+        b = cur["bt"]
+        if b is None:
             return
         for p in dp:
             p.zero_()
         for i in range(len(loc)):
-            bt.set_coeffs_device(i, dd[i], du[i])
-        res["b"] = bt.solve_device(dp, db, o)
+            b.set_coeffs_device(i, dd[i], du[i])
+        res["b"] = b.solve_device(dp, db, o)
 
     def timed(fn, k):
         barrier(ws)
@@ -311,14 +320,19 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
     batched()
     ms_b = timed(batched, steps) / steps
     res_graph = res["b"]
-    # the same batch with the inner loop of all systems in one persistent
-    # (cooperative) launch per restart
+    # every system in the one-launch-per-phase batch, graph loop and one
+    # persistent (cooperative) launch per restart
+    cur["bt"] = bt_one
+    batched()
+    res_one = res["b"]
+    ms_b1 = timed(batched, steps) / steps
     o_graph = o
     o = _lib.default_options(persistentMaxCells=1 << 30, **opts)
     batched()
     res_persist = res["b"]
     ms_bp = timed(batched, steps) / steps
     o = o_graph
+    cur["bt"] = bt
     res["b"] = res_graph
     ctxs = []
     for s in loc:
@@ -384,8 +398,9 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
         many_same[precond] = all(p.nIterations == q for p, q in zip(res.get("m", []), its))
     for c in ctxs:
         c.close()
-    if bt is not None:
-        bt.close()
+    for b in (bt, bt_one):
+        if b is not None:
+            b.close()
     recs = shard.gather_records(mine, [shard.perf_record(p) for p in res["b"]], S, rank, ws)
     same = shard.gather_records(mine, [{"same": int(p.nIterations == q)} for p, q in
                                        zip(res["b"], it_p)], S, rank, ws)
@@ -405,15 +420,24 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
             "plain_loop_solves_per_s": round(S / (ms_p / 1e3), 2),
             "host_sync_loop_solves_per_s": round(S / (ms_h / 1e3), 2),
             "speedup_vs_plain_loop": round(ms_p / ms_b, 3),
+            "batched_note": "batched = cf_batch_solve as the library runs it: systems of at "
+                            "least numSMs x 2048 cells (%d of %d here) as single solves on "
+                            "their own streams, concurrently with one launch per phase for "
+                            "the rest" % (sum(1 for s in systems if s.n >= solo_min), S),
+            "one_launch_per_phase": {
+                "note": "every system in the one-launch-per-phase batch (solo cells -1)",
+                "ms": round(ms_b1, 2), "solves_per_s": round(S / (ms_b1 / 1e3), 2),
+                "speedup_vs_plain_loop": round(ms_p / ms_b1, 3),
+                "speedup_vs_host_sync_loop": round(ms_h / ms_b1, 3)},
             "persistent_launch": {
-                "note": "the batched solve with the inner loop of all systems as one "
+                "note": "every system in the batch, the inner loop of all systems as one "
                         "cooperative launch per restart (persistentMaxCells), bounded grid "
                         "barriers between phases; results bit-identical to the graph loop",
                 "ms": round(ms_bp, 2), "solves_per_s": round(S / (ms_bp / 1e3), 2),
                 "speedup_vs_plain_loop": round(ms_p / ms_bp, 3),
                 "speedup_vs_host_sync_loop": round(ms_h / ms_bp, 3),
                 "iterations_identical": [p.nIterations for p in res_persist] ==
-                                        [p.nIterations for p in res_graph]},
+                                        [p.nIterations for p in res_one]},
             "speedup_vs_host_sync_loop": round(ms_h / ms_b, 3),
             "ms": {"batched": round(ms_b, 2), "plain": round(ms_p, 2),
                    "host_sync": round(ms_h, 2)},
