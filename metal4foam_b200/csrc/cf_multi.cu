@@ -54,10 +54,7 @@ constexpr int RMAX = 4;
 struct MBufs
 {
     long long n;            // stride between components
-    long long N;            // n * R: stride between parities / correction buffers
-    float *rA, *rA0, *yA, *sA, *zA, *tA;                 // [R][n]
-    float *P, *AyA;         // [2][R][n]: by iteration parity, as the single solve's
-    float* D;               // [3][R][n]
+    float *rA, *rA0, *P, *yA, *AyA, *sA, *zA, *tA, *D;   // D: [3][R][n]
     double *psi, *b, *r64;
     const float* diag;
     const float* rD;
@@ -309,57 +306,6 @@ __global__ void km_setup(InnerState* st, const double* target, const int* maxIte
     q.ticket = 0u;
 }
 
-// R FP32 rows of A x sharing the entry loads, x formed per column: X(c, xr)
-// fills xr[r] for every component r that is on.  Same columns, same order and
-// same operations per component as row_f32 (either column stream).
-template <int R, int MAXW, class XC>
-__device__ __forceinline__ void rows_f32_fused(const DevSell& A, int row, float (&acc)[R],
-                                               const bool (&on)[R], XC X)
-{
-    const int sl = row >> 5;
-    const int b0 = A.ellW ? sl * SLICE * A.ellW : __ldg(A.sliceOff + sl);
-    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + sl + 1) - b0) >> 5;
-    const int base = b0 + (row & 31);
-    for (int k0 = 0; k0 < w; k0 += MAXW)
-    {
-        int cc[MAXW];
-        float v[MAXW];
-#pragma unroll
-        for (int k = 0; k < MAXW; ++k)
-        {
-            const int e = base + SLICE * (k0 + k);
-            cc[k] = -1;
-            v[k] = 0.0f;
-            if (k0 + k < w)
-            {
-                if (A.col16)
-                {
-                    const short o = __ldcs(A.col16 + e);
-                    cc[k] = o == COL16_PAD ? -1 : row + o;
-                }
-                else
-                {
-                    const int c = __ldcs(A.col + e);
-                    cc[k] = c == -1 ? -1 : col_index(c);
-                }
-                v[k] = __ldcs(A.val + e);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < MAXW; ++k)
-        {
-            if (cc[k] == -1) continue;
-            float xr[R];
-            X(cc[k], xr);
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (on[r]) acc[r] = __fadd_rn(acc[r], __fmul_rn(v[k], xr[r]));
-        }
-    }
-}
-
-// Start of the inner BiCGStab per component (k_bicg_init): rA = rA0 = float
-// r64, delta = p = AyA = 0 in both parities; rA0.rA; beta = 0.
 template <int R>
 __global__ void __launch_bounds__(NT) km_bicg_init(int n, MBufs M)
 {
@@ -381,9 +327,7 @@ __global__ void __launch_bounds__(NT) km_bicg_init(int n, MBufs M)
             M.rA0[i] = ra;
             M.D[i] = 0.0f;           // buffer 0 of component r
             M.P[i] = 0.0f;
-            M.P[M.N + i] = 0.0f;
             M.AyA[i] = 0.0f;
-            M.AyA[M.N + i] = 0.0f;
             acc[r] += (double)ra * (double)ra;
         }
     }
@@ -400,65 +344,57 @@ __global__ void __launch_bounds__(NT) km_bicg_init(int n, MBufs M)
     }
 }
 
-// k_bicg_ab for R components: p = rA + beta (p_old - omega AyA_old) and
-// yA = rD p formed at every gathered column (the previous iteration's p and
-// AyA sit in the other parity); writes p, yA, AyA = A yA for the own row;
-// rA0.AyA -> alpha per component.
-template <int R, int MAXW>
-__global__ void __launch_bounds__(NT) km_bicg_ab(DevSell A, MBufs M)
+template <int R>
+__global__ void __launch_bounds__(NT) km_bicg_a(int n, MBufs M)
 {
     bool on[R];
     float beta[R], omega[R];
-    size_t oldOff[R], newOff[R];   // parity blocks of P and AyA, per component
     load_on<R>(M.st, on);
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         beta[r] = (float)M.st[r].beta;
         omega[r] = (float)M.st[r].omega;
-        const int par = M.st[r].it & 1;
-        oldOff[r] = (size_t)(par ^ 1) * M.N + (size_t)r * M.n;
-        newOff[r] = (size_t)par * M.N + (size_t)r * M.n;
     }
-    const float* __restrict__ P = M.P;
-    const float* __restrict__ Ay = M.AyA;
-    const float* __restrict__ rA = M.rA;
-    const float* __restrict__ rD = M.rD;
-    auto pf = [&](int r, int c) {
-        return __fadd_rn(__ldg(rA + (size_t)r * M.n + c),
-                         __fmul_rn(beta[r], __fsub_rn(__ldg(P + oldOff[r] + c),
-                                                      __fmul_rn(omega[r], __ldg(Ay + oldOff[r] + c)))));
-    };
+    CF_ROWS(row, n)
+    {
+        const float rd = M.rD[row];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (!on[r]) continue;
+            const size_t i = (size_t)r * M.n + row;
+            const float p = __fadd_rn(M.rA[i],
+                                      __fmul_rn(beta[r], __fsub_rn(M.P[i], __fmul_rn(omega[r], M.AyA[i]))));
+            M.P[i] = p;
+            M.yA[i] = __fmul_rn(rd, p);
+        }
+    }
+}
+
+template <int R, int MAXW>
+__global__ void __launch_bounds__(NT) km_bicg_b(DevSell A, MBufs M)
+{
+    bool on[R];
+    load_on<R>(M.st, on);
     double acc[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r] = 0.0;
+    const float* __restrict__ yA = M.yA;
     CF_ROWS(row, A.n)
     {
-        const float rd = rD[row];
+        float y[R];
         const float dg = M.diag[row];
-        float v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-        {
-            v[r] = 0.0f;
-            if (!on[r]) continue;
-            const float p = pf(r, row);
-            const float y = __fmul_rn(rd, p);
-            M.P[newOff[r] + row] = p;
-            M.yA[(size_t)r * M.n + row] = y;
-            v[r] = __fmul_rn(dg, y);
-        }
-        rows_f32_fused<R, MAXW>(A, row, v, on, [&](int c, float (&xr)[R]) {
-            const float rdc = __ldg(rD + c);
-#pragma unroll
-            for (int r = 0; r < R; ++r) xr[r] = on[r] ? __fmul_rn(rdc, pf(r, c)) : 0.0f;
-        });
+        for (int r = 0; r < R; ++r) y[r] = __fmul_rn(dg, yA[(size_t)r * M.n + row]);
+        rows_f32<R, MAXW>(A, row, y, on, [&](int r, int c) { return __ldg(yA + (size_t)r * M.n + c); });
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
             if (!on[r]) continue;
-            M.AyA[newOff[r] + row] = v[r];
-            acc[r] += (double)M.rA0[(size_t)r * M.n + row] * (double)v[r];
+            const size_t i = (size_t)r * M.n + row;
+            M.AyA[i] = y[r];
+            acc[r] += (double)M.rA0[i] * (double)y[r];
         }
     }
     if (grid_sum<R>(acc, M.part, M.ticket) && threadIdx.x == 0)
@@ -474,69 +410,33 @@ __global__ void __launch_bounds__(NT) km_bicg_ab(DevSell A, MBufs M)
     }
 }
 
-// k_bicg_cd for R components: s = rA - alpha AyA and zA = rD s formed at
-// every gathered column; writes sA, zA, tA = A zA for the own row; sum|s|,
-// s.tA, tA.tA; then per component the breakdown test, the |s| early exit and
-// omega (the host checks of metalFoamBackend.C:829-866).
-template <int R, int MAXW>
-__global__ void __launch_bounds__(NT) km_bicg_cd(DevSell A, MBufs M, cudaGraphConditionalHandle h,
-                                                 int useCond)
+template <int R>
+__global__ void __launch_bounds__(NT) km_bicg_c(int n, MBufs M, cudaGraphConditionalHandle h,
+                                                int useCond)
 {
     bool on[R];
     float alpha[R];
-    size_t aOff[R];   // this iteration's AyA block of each component
     load_on<R>(M.st, on);
 #pragma unroll
-    for (int r = 0; r < R; ++r)
-    {
-        alpha[r] = (float)M.st[r].alpha;
-        aOff[r] = (size_t)(M.st[r].it & 1) * M.N + (size_t)r * M.n;
-    }
-    const float* __restrict__ Ay = M.AyA;
-    const float* __restrict__ rA = M.rA;
-    const float* __restrict__ rD = M.rD;
-    double acc[3 * R];
+    for (int r = 0; r < R; ++r) alpha[r] = (float)M.st[r].alpha;
+    double acc[R];
 #pragma unroll
-    for (int r = 0; r < 3 * R; ++r) acc[r] = 0.0;
-    CF_ROWS(row, A.n)
+    for (int r = 0; r < R; ++r) acc[r] = 0.0;
+    CF_ROWS(row, n)
     {
-        const float rd = rD[row];
-        const float dg = M.diag[row];
-        float t[R], sv[R];
+        const float rd = M.rD[row];
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
-            t[r] = 0.0f;
-            sv[r] = 0.0f;
             if (!on[r]) continue;
             const size_t i = (size_t)r * M.n + row;
-            sv[r] = __fsub_rn(rA[i], __fmul_rn(alpha[r], Ay[aOff[r] + row]));
-            const float z = __fmul_rn(rd, sv[r]);
-            M.sA[i] = sv[r];
-            M.zA[i] = z;
-            acc[3 * r] += (double)fabsf(sv[r]);
-            t[r] = __fmul_rn(dg, z);
-        }
-        rows_f32_fused<R, MAXW>(A, row, t, on, [&](int c, float (&xr)[R]) {
-            const float rdc = __ldg(rD + c);
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-            {
-                xr[r] = on[r] ? __fmul_rn(rdc, __fsub_rn(__ldg(rA + (size_t)r * M.n + c),
-                                                         __fmul_rn(alpha[r], __ldg(Ay + aOff[r] + c))))
-                              : 0.0f;
-            }
-        });
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-        {
-            if (!on[r]) continue;
-            M.tA[(size_t)r * M.n + row] = t[r];
-            acc[3 * r + 1] += (double)sv[r] * (double)t[r];
-            acc[3 * r + 2] += (double)t[r] * (double)t[r];
+            const float sv = __fsub_rn(M.rA[i], __fmul_rn(alpha[r], M.AyA[i]));
+            M.sA[i] = sv;
+            M.zA[i] = __fmul_rn(rd, sv);
+            acc[r] += (double)fabsf(sv);
         }
     }
-    if (grid_sum<3 * R>(acc, M.part, M.ticket) && threadIdx.x == 0)
+    if (grid_sum<R>(acc, M.part, M.ticket) && threadIdx.x == 0)
     {
         int left = 0;
 #pragma unroll
@@ -545,7 +445,7 @@ __global__ void __launch_bounds__(NT) km_bicg_cd(DevSell A, MBufs M, cudaGraphCo
             InnerState& q = M.st[r];
             if (on[r])
             {
-                q.resS = acc[3 * r];
+                q.resS = acc[r];
                 if (!isfinite(q.rA0rA) || !isfinite(q.alpha) || !isfinite(q.resS))
                 {
                     q.singular = 1;
@@ -556,12 +456,6 @@ __global__ void __launch_bounds__(NT) km_bicg_cd(DevSell A, MBufs M, cudaGraphCo
                     q.early = 1;
                     q.done = 1;
                 }
-                else
-                {
-                    q.tAsA = acc[3 * r + 1];
-                    q.tAtA = acc[3 * r + 2];
-                    q.omega = q.tAsA / q.tAtA;
-                }
             }
             left += q.done ? 0 : 1;
         }
@@ -569,15 +463,13 @@ __global__ void __launch_bounds__(NT) km_bicg_cd(DevSell A, MBufs M, cudaGraphCo
     }
 }
 
-// k_bicg_e for R components: delta += alpha yA + omega zA, rA = s - omega
-// tA, sum|rA| and rA0.rA (beta), the end-of-iteration checks; components
-// flagged early by km_bicg_cd take delta += alpha yA instead and end.
-template <int R>
-__global__ void __launch_bounds__(NT) km_bicg_e(int n, MBufs M, cudaGraphConditionalHandle h,
-                                                int useCond)
+// early exits: delta += alpha yA (components flagged early in km_bicg_c, not
+// yet applied); the rest: tA = A zA with sA.tA and tA.tA -> omega
+template <int R, int MAXW>
+__global__ void __launch_bounds__(NT) km_bicg_d(DevSell A, MBufs M)
 {
     bool on[R], ear[R];
-    float alpha[R], omega[R];
+    float alpha[R];
     int cur[R], nxt[R];
 #pragma unroll
     for (int r = 0; r < R; ++r)
@@ -585,6 +477,73 @@ __global__ void __launch_bounds__(NT) km_bicg_e(int n, MBufs M, cudaGraphConditi
         const InnerState& q = M.st[r];
         on[r] = !q.done;
         ear[r] = q.early && !q.converged;
+        alpha[r] = (float)q.alpha;
+        cur[r] = q.cur;
+        nxt[r] = q.nxt;
+    }
+    double acc[2 * R];
+#pragma unroll
+    for (int r = 0; r < 2 * R; ++r) acc[r] = 0.0;
+    const float* __restrict__ zA = M.zA;
+    CF_ROWS(row, A.n)
+    {
+        float t[R];
+        const float dg = M.diag[row];
+#pragma unroll
+        for (int r = 0; r < R; ++r) t[r] = __fmul_rn(dg, zA[(size_t)r * M.n + row]);
+        rows_f32<R, MAXW>(A, row, t, on, [&](int r, int c) { return __ldg(zA + (size_t)r * M.n + c); });
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            const size_t i = (size_t)r * M.n + row;
+            if (on[r])
+            {
+                M.tA[i] = t[r];
+                acc[2 * r] += (double)M.sA[i] * (double)t[r];
+                acc[2 * r + 1] += (double)t[r] * (double)t[r];
+            }
+            else if (ear[r])
+            {
+                M.D[((size_t)nxt[r] * R + r) * M.n + row] =
+                    __fadd_rn(M.D[((size_t)cur[r] * R + r) * M.n + row], __fmul_rn(alpha[r], M.yA[i]));
+            }
+        }
+    }
+    if (grid_sum<2 * R>(acc, M.part, M.ticket) && threadIdx.x == 0)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            InnerState& q = M.st[r];
+            if (on[r])
+            {
+                q.tAsA = acc[2 * r];
+                q.tAtA = acc[2 * r + 1];
+                q.omega = q.tAsA / q.tAtA;
+            }
+            else if (ear[r])
+            {
+                q.cur = q.nxt;
+                q.it = q.it + 1;
+                q.finalResSum = q.resS;
+                q.converged = 1;
+            }
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(NT) km_bicg_e(int n, MBufs M, cudaGraphConditionalHandle h,
+                                                int useCond)
+{
+    bool on[R];
+    float alpha[R], omega[R];
+    int cur[R], nxt[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        const InnerState& q = M.st[r];
+        on[r] = !q.done;
         alpha[r] = (float)q.alpha;
         omega[r] = (float)q.omega;
         cur[r] = q.cur;
@@ -598,22 +557,16 @@ __global__ void __launch_bounds__(NT) km_bicg_e(int n, MBufs M, cudaGraphConditi
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
+            if (!on[r]) continue;
             const size_t i = (size_t)r * M.n + row;
-            const float* Dc = M.D + (size_t)cur[r] * M.N + (size_t)r * M.n;
-            float* Dn = M.D + (size_t)nxt[r] * M.N + (size_t)r * M.n;
-            if (on[r])
-            {
-                Dn[row] = __fadd_rn(Dc[row], __fadd_rn(__fmul_rn(alpha[r], M.yA[i]),
-                                                       __fmul_rn(omega[r], M.zA[i])));
-                const float rv = __fsub_rn(M.sA[i], __fmul_rn(omega[r], M.tA[i]));
-                M.rA[i] = rv;
-                acc[2 * r] += (double)fabsf(rv);
-                acc[2 * r + 1] += (double)M.rA0[i] * (double)rv;
-            }
-            else if (ear[r])
-            {
-                Dn[row] = __fadd_rn(Dc[row], __fmul_rn(alpha[r], M.yA[i]));
-            }
+            const float* Dc = M.D + ((size_t)cur[r] * R + r) * M.n;
+            float* Dn = M.D + ((size_t)nxt[r] * R + r) * M.n;
+            Dn[row] = __fadd_rn(Dc[row], __fadd_rn(__fmul_rn(alpha[r], M.yA[i]),
+                                                   __fmul_rn(omega[r], M.zA[i])));
+            const float rv = __fsub_rn(M.sA[i], __fmul_rn(omega[r], M.tA[i]));
+            M.rA[i] = rv;
+            acc[2 * r] += (double)fabsf(rv);
+            acc[2 * r + 1] += (double)M.rA0[i] * (double)rv;
         }
     }
     if (grid_sum<2 * R>(acc, M.part, M.ticket) && threadIdx.x == 0)
@@ -632,13 +585,6 @@ __global__ void __launch_bounds__(NT) km_bicg_e(int n, MBufs M, cudaGraphConditi
                 q.rA0rAold = q.rA0rA;
                 q.rA0rA = acc[2 * r + 1];
                 q.beta = (q.rA0rA / q.rA0rAold) * (q.alpha / q.omega);
-            }
-            else if (ear[r])
-            {
-                q.cur = q.nxt;
-                q.it = q.it + 1;
-                q.finalResSum = q.resS;
-                q.converged = 1;
             }
             left += q.done ? 0 : 1;
         }
@@ -705,11 +651,11 @@ int ensure_multi(cf_context* c)
     c->multi = m;
     m->n = c->n;
     const size_t N = (size_t)c->n * RMAX;
-    // the kernels reduce up to 3 R values per launch; grid_for never returns
+    // the kernels reduce up to 2 R values per launch; grid_for never returns
     // more than numSMs * maxBlocksPerSM blocks
-    const size_t partCount = (size_t)3 * RMAX * c->numSMs * c->maxBlocksPerSM;
-    // rA rA0 yA sA zA tA (6) + P, AyA (2 parities each) + D (3)
-    if (cudaMalloc((void**)&m->f, sizeof(float) * N * 13) != cudaSuccess ||
+    const size_t partCount = (size_t)2 * RMAX * c->numSMs * c->maxBlocksPerSM;
+    // rA rA0 P yA AyA sA zA tA (8) + D (3)
+    if (cudaMalloc((void**)&m->f, sizeof(float) * N * 11) != cudaSuccess ||
         cudaMalloc((void**)&m->d, sizeof(double) * N * 3) != cudaSuccess ||
         cudaMalloc((void**)&m->part, sizeof(double) * partCount) != cudaSuccess ||
         cudaMalloc((void**)&m->st, sizeof(InnerState) * RMAX) != cudaSuccess ||
@@ -729,7 +675,7 @@ int ensure_multi(cf_context* c)
     }
     CF_CUDA(cudaMemset(m->st, 0, sizeof(InnerState) * RMAX));
     CF_CUDA(cudaMemset(m->drv, 0, sizeof(DriverState) * RMAX));
-    CF_CUDA(cudaMemset(m->f, 0, sizeof(float) * N * 13));
+    CF_CUDA(cudaMemset(m->f, 0, sizeof(float) * N * 11));
     return CF_OK;
 }
 
@@ -740,16 +686,15 @@ MBufs mbufs(cf_context* c, int R)
     MBufs M;
     M.n = c->n;
     float* f = m->f;
-    M.N = (long long)N;
     M.rA = f;
     M.rA0 = f + N;
-    M.yA = f + 2 * N;
-    M.sA = f + 3 * N;
-    M.zA = f + 4 * N;
-    M.tA = f + 5 * N;
-    M.P = f + 6 * N;
-    M.AyA = f + 8 * N;
-    M.D = f + 10 * N;
+    M.P = f + 2 * N;
+    M.yA = f + 3 * N;
+    M.AyA = f + 4 * N;
+    M.sA = f + 5 * N;
+    M.zA = f + 6 * N;
+    M.tA = f + 7 * N;
+    M.D = f + 8 * N;
     M.psi = m->d;
     M.b = m->d + N;
     M.r64 = m->d + 2 * N;
@@ -771,13 +716,22 @@ int launch_multi_body(cf_context* c, cudaGraphConditionalHandle h, int useCond)
     const MBufs M = mbufs(c, R);
     cudaStream_t s = c->stream;
     const int n = c->n;
-    // every pass runs on the grid of its single-solve counterpart, so every
-    // component's sums fold exactly as the single solve's
+    // grids of the single-solve kernels (same reduction order per
+    // component).  The single solve fuses a into b and c into d (p, yA and
+    // s, zA formed at every gathered column); here the five passes stay
+    // separate -- recomputing them for every component at every gathered
+    // column measured 9% slower at 64^3 x 3 -- and each pass runs on the
+    // grid of the fused kernel that contains it, so every component's sums
+    // fold exactly as the single solve's
     const int gab = grid_for(c, (const void*)k_bicg_ab<MW>, n);
     const int gcd = grid_for(c, (const void*)k_bicg_cd<MW>, n);
-    km_bicg_ab<R, MW><<<gab, NT, 0, s>>>(A, M);
+    km_bicg_a<R><<<gab, NT, 0, s>>>(n, M);
     CF_LAUNCH();
-    km_bicg_cd<R, MW><<<gcd, NT, 0, s>>>(A, M, h, useCond);
+    km_bicg_b<R, MW><<<gab, NT, 0, s>>>(A, M);
+    CF_LAUNCH();
+    km_bicg_c<R><<<gcd, NT, 0, s>>>(n, M, h, useCond);
+    CF_LAUNCH();
+    km_bicg_d<R, MW><<<gcd, NT, 0, s>>>(A, M);
     CF_LAUNCH();
     km_bicg_e<R><<<grid_for(c, (const void*)k_bicg_e, n), NT, 0, s>>>(n, M, h, useCond);
     CF_LAUNCH();
