@@ -97,6 +97,8 @@ void free_topology(cf_context* c)
     c->n = c->nf = 0;
     c->lastLow = c->lastUpp = nullptr;
     c->d_col16 = nullptr;
+    c->d_pcol16 = nullptr;
+    c->d_pval32 = nullptr;
 }
 
 // Validate the five lduAddressing arrays (the bounds check the reference
@@ -351,6 +353,11 @@ DevSell sell_of(const cf_context* c)
     A.val = c->d_val32;
     A.val64 = c->d_val64;
     A.col16 = c->cfgIndexBits == 16 ? c->d_col16 : nullptr;
+    if (A.col16 && c->d_pcol16 && c->ellW > 0)
+    {
+        A.pcol16 = c->d_pcol16;
+        A.pval = c->d_pval32;
+    }
     A.ellW = c->ellW;
     return A;
 }
@@ -645,6 +652,7 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
     // lies within 32767 rows of its row (the host copy lives until the
     // synchronisation below)
     std::vector<short> col16((size_t)std::max(nnzp, 1LL), COL16_PAD);
+    std::vector<short> pcol16;
     {
         bool fits = true;
         for (int32_t sl = 0; sl < nslices && fits; ++sl)
@@ -670,6 +678,25 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
             CF_TRY(dalloc(c, &c->d_col16, col16.size()));
             CF_CUDA(cudaMemcpyAsync(c->d_col16, col16.data(), sizeof(short) * col16.size(),
                                     cudaMemcpyHostToDevice, c->stream));
+            // the same stream in the paired order, with a paired copy of the
+            // FP32 values (staged with them), when every slice has one width
+            if (L.uniformW > 0)
+            {
+                const int W = L.uniformW;
+                const long long sw = (long long)SLICE * W;
+                pcol16.assign(col16.size(), COL16_PAD);
+                for (long long e = 0; e < nnzp; ++e)
+                {
+                    const long long sl = e / sw;
+                    const int rem = (int)(e - sl * sw);
+                    pcol16[pair_index(sl * sw, W, rem / SLICE, rem % SLICE)] = col16[e];
+                }
+                CF_TRY(dalloc(c, &c->d_pcol16, pcol16.size()));
+                CF_TRY(dalloc(c, &c->d_pval32, pcol16.size()));
+                CF_CUDA(cudaMemcpyAsync(c->d_pcol16, pcol16.data(),
+                                        sizeof(short) * pcol16.size(), cudaMemcpyHostToDevice,
+                                        c->stream));
+            }
         }
     }
     // locality of the cluster PCG's row split (cf_cluster.cu): the share of
@@ -717,6 +744,12 @@ int stage_vals(cf_context* c, int sym32)
     k_stage_vals<<<g, NT, 0, c->stream>>>(c->nnzp, c->d_col, c->d_eface, up, lo, sym32,
                                           c->d_val32, c->d_val64, c->d_valT64);
     CF_LAUNCH();
+    if (c->d_pval32)
+    {
+        k_pair_vals<<<grid_for(c, (const void*)k_pair_vals, c->nnzp), NT, 0, c->stream>>>(
+            c->nnzp, c->ellW, c->d_val32, c->d_pval32);
+        CF_LAUNCH();
+    }
     c->val32Sym = sym32;
     if (c->lduReady) CF_TRY(stage_face32(c, up, lo, sym32));
     return CF_OK;

@@ -44,6 +44,8 @@ struct cf_context
     int* d_sliceOff = nullptr;
     int* d_col = nullptr;
     short* d_col16 = nullptr;              // row-relative columns, when they fit in 16 bits
+    short* d_pcol16 = nullptr;             // d_col16 in the paired order (uniform width)
+    float* d_pval32 = nullptr;             // d_val32 in the paired order
     int* d_eface = nullptr;
     int* d_perm = nullptr;
     int* d_low = nullptr;

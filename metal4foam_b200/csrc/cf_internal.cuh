@@ -43,6 +43,18 @@ constexpr double VSMALL = 1.0e-300;
 // SpMVs and names the same columns, so every sum is unchanged.
 constexpr short COL16_PAD = -32768;
 
+// Paired order of a uniform-width (W) SELL slice starting at sliceBase:
+// lane l's entries 2g and 2g+1 sit side by side (one 4-byte column pair, one
+// 8-byte value pair per lane, 256 contiguous bytes of values per warp and
+// pair), the last entry of an odd width alone.  Same entries as the
+// column-major order, read with half the load instructions.
+__host__ __device__ inline long long pair_index(long long sliceBase, int W, int k, int lane)
+{
+    const int even = W & ~1;
+    return k < even ? sliceBase + 64LL * (k >> 1) + 2 * lane + (k & 1)
+                    : sliceBase + 32LL * even + lane;
+}
+
 struct DevSell
 {
     int n;                          // rows
@@ -54,6 +66,8 @@ struct DevSell
     const short* col16 = nullptr;   // [nnz_padded] row-relative columns, or null
     int ellW = 0;                   // > 0: every slice has this width and slice s
                                     // starts at 32 s ellW (no sliceOff load)
+    const short* pcol16 = nullptr;  // col16 in the paired order (uniform width only),
+    const float* pval = nullptr;    // val in the paired order: the FP32 row reads these
 };
 
 // State of one inner solve (metalFoamBackend::Stats plus the device scalars

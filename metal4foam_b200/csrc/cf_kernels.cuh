@@ -232,7 +232,10 @@ __device__ __forceinline__ int col_index(int c) { return c & 0x7fffffff; }
 
 // One FP32 row of A x: acc (= diag*x_row) plus the entries in stored order
 // (owner side, then neighbour side), as ldu_spmv (metalFoamKernels.metal:131-147).
-template <int MAXW, class XF>
+// PAIRED = 1 reads the paired copy of the compact stream (A.pcol16/A.pval,
+// uniform width); PAIRED = 0 the column-major streams.  A kernel is compiled
+// for one of the two, so neither pays registers for the other.
+template <int MAXW, int PAIRED = 0, class XF>
 __device__ __forceinline__ float row_f32(const DevSell& A, int row, float acc,
                                          XF xf)
 {
@@ -240,6 +243,61 @@ __device__ __forceinline__ float row_f32(const DevSell& A, int row, float acc,
     const int b0 = A.ellW ? s * SLICE * A.ellW : __ldg(A.sliceOff + s);
     const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + s + 1) - b0) >> 5;
     const int base = b0 + (row & 31);
+    if constexpr (PAIRED != 0)
+    {
+        // paired order (uniform width): one short2 and one float2 load per
+        // two entries; same entries, summed in the same order (entry
+        // offsets fit 32 bits: the layout is refused beyond 2^31 entries)
+        const int lane = row & 31;
+        const int sb = s * SLICE * w;
+        if (w <= MAXW)
+        {
+            short o[MAXW];
+            float v[MAXW];
+            const int even = w & ~1;
+#pragma unroll
+            for (int g = 0; g < MAXW / 2; ++g)
+            {
+                o[2 * g] = o[2 * g + 1] = COL16_PAD;
+                v[2 * g] = v[2 * g + 1] = 0.0f;
+                if (2 * g < even)
+                {
+                    const int e = sb + 64 * g + 2 * lane;
+                    const short2 oo = __ldcs(reinterpret_cast<const short2*>(A.pcol16 + e));
+                    const float2 vv = __ldcs(reinterpret_cast<const float2*>(A.pval + e));
+                    o[2 * g] = oo.x;
+                    o[2 * g + 1] = oo.y;
+                    v[2 * g] = vv.x;
+                    v[2 * g + 1] = vv.y;
+                }
+                else if (2 * g < w)
+                {
+                    const int e = sb + 32 * even + lane;   // the last entry of an odd width
+                    o[2 * g] = __ldcs(A.pcol16 + e);
+                    v[2 * g] = __ldcs(A.pval + e);
+                }
+            }
+            float x[MAXW];
+#pragma unroll
+            for (int k = 0; k < MAXW; ++k) x[k] = (o[k] != COL16_PAD) ? xf(row + o[k]) : 0.0f;
+#pragma unroll
+            for (int k = 0; k < MAXW; ++k)
+                if (o[k] != COL16_PAD) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
+        }
+        else
+        {
+            for (int k = 0; k < w; ++k)
+            {
+                const int e = (int)pair_index(sb, w, k, lane);
+                const short o = __ldcs(A.pcol16 + e);
+                if (o != COL16_PAD)
+                    acc = __fadd_rn(acc, __fmul_rn(__ldcs(A.pval + e), xf(row + o)));
+            }
+        }
+        return acc;
+    }
+    else
+    {
     if (A.col16)
     {
         // compact index stream: same columns, same order, half the bytes
@@ -315,6 +373,7 @@ __device__ __forceinline__ float row_f32(const DevSell& A, int row, float acc,
         }
     }
     return acc;
+    }
 }
 
 // One FP64 row: acc (= diag*x_row) plus neighbour-side entries, then
@@ -408,6 +467,20 @@ static __global__ void k_stage_vals(long long nnzp, const int* __restrict__ col,
         val64[e] = a;
         valT64[e] = nbr ? u : l;
         val32[e] = (float)((sym32 && nbr) ? u : a);
+    }
+}
+
+// val32 in the paired order of a uniform-width-W layout (see pair_index)
+static __global__ void k_pair_vals(long long nnzp, int W, const float* __restrict__ val32,
+                                   float* __restrict__ pval)
+{
+    const long long sw = (long long)SLICE * W;
+    for (long long e = (long long)blockIdx.x * NT + threadIdx.x; e < nnzp;
+         e += (long long)gridDim.x * NT)
+    {
+        const long long s = e / sw;
+        const int rem = (int)(e - s * sw);
+        pval[pair_index(s * sw, W, rem / SLICE, rem % SLICE)] = val32[e];
     }
 }
 
@@ -761,8 +834,8 @@ static __global__ void __launch_bounds__(NT) k_pcg_init(PcgBufs B, const double*
 // encoded per step at metalFoamBackend.C:365-384) fused into one pass:
 //   v = A z_{j-1};  w = c2 w + c3 rD (r - v);  z_j = z_{j-1} + w.
 // On the last step the z.r dot and reduce_scalars mode 0 (wArA, beta) follow.
-template <bool LAST, int MAXW>
-static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
+template <bool LAST, int MAXW, int PAIRED = 0>
+static __global__ void __launch_bounds__(NT, PAIRED ? 8 : 0) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
                                                   const float* win, float* wout, float* zout,
                                                   int j, InnerState* st, double* part)
 {
@@ -773,7 +846,7 @@ static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, c
     CF_ROWS(row, A.n)
     {
         const float zr = zin[row];
-        const float v = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], zr),
+        const float v = row_f32<MAXW, PAIRED>(A, row, __fmul_rn(B.diag[row], zr),
                                       [&](int c) { return __ldg(zin + c); });
         const float r = B.rA[row];
         const float wn = __fadd_rn(__fmul_rn(c2, win[row]),
@@ -794,11 +867,13 @@ static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, c
     }
 }
 
-// pcg_update_p fused into ldu_spmv_dotw (metalFoamKernels.metal:64-109,237-247):
+// pcg_update_p fused into ldu_spmv_dotw (metalFoamKernels.metal:64-109,237-247)
+// (launched with the column-major streams: its p-update at every gathered
+// column needs more registers than the paired loads leave at full occupancy):
 // p_new = wA + beta p_old is formed on the fly for every gathered column, so
 // p never needs its own pass; writes p_new, q = A p_new; p.q -> alpha
 // (reduce_scalars mode 1).
-template <int MAXW>
+template <int MAXW, int PAIRED = 0>
 static __global__ void __launch_bounds__(NT) k_pcg_p_spmv(DevSell A, PcgBufs B, const float* wA,
                                                    InnerState* st, double* part)
 {
@@ -813,7 +888,7 @@ static __global__ void __launch_bounds__(NT) k_pcg_p_spmv(DevSell A, PcgBufs B, 
     CF_ROWS(row, n)
     {
         const float pr = pf(row);
-        const float y = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], pr), pf);
+        const float y = row_f32<MAXW, PAIRED>(A, row, __fmul_rn(B.diag[row], pr), pf);
         Pn[row] = pr;
         B.Q[row] = y;
         acc[0] += (double)pr * (double)y;
@@ -996,7 +1071,7 @@ static __global__ void __launch_bounds__(NT) k_bicg_init(BicgBufs B, const doubl
 // column (the previous iteration's p and AyA sit in the other parity), so
 // they need no pass of their own; writes p, yA, AyA = A yA for the own row;
 // rA0.AyA -> alpha.
-template <int MAXW>
+template <int MAXW, int PAIRED = 0>
 static __global__ void __launch_bounds__(NT) k_bicg_ab(DevSell A, BicgBufs B, InnerState* st,
                                                 double* part)
 {
@@ -1021,7 +1096,7 @@ static __global__ void __launch_bounds__(NT) k_bicg_ab(DevSell A, BicgBufs B, In
         const float y = __fmul_rn(B.rD[row], p);
         Pn[row] = p;
         B.yA[row] = y;
-        const float v = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], y), yf);
+        const float v = row_f32<MAXW, PAIRED>(A, row, __fmul_rn(B.diag[row], y), yf);
         An[row] = v;
         acc[0] += (double)B.rA0[row] * (double)v;
     }
@@ -1038,7 +1113,7 @@ static __global__ void __launch_bounds__(NT) k_bicg_ab(DevSell A, BicgBufs B, In
 // row; sum|s|, s.tA and tA.tA in one reduction.  The finaliser applies the
 // host checks of metalFoamBackend.C:829-866 first -- breakdown on rA0rA /
 // alpha / sum|s|, the |s| early exit -- and only then omega = s.tA / tA.tA.
-template <int MAXW>
+template <int MAXW, int PAIRED = 0>
 static __global__ void __launch_bounds__(NT) k_bicg_cd(DevSell A, BicgBufs B, InnerState* st,
                                                 double* part, cudaGraphConditionalHandle h,
                                                 int useCond)
@@ -1059,7 +1134,7 @@ static __global__ void __launch_bounds__(NT) k_bicg_cd(DevSell A, BicgBufs B, In
         B.sA[row] = sv;
         B.zA[row] = z;
         acc[0] += (double)fabsf(sv);
-        const float t = row_f32<MAXW>(A, row, __fmul_rn(B.diag[row], z), zf);
+        const float t = row_f32<MAXW, PAIRED>(A, row, __fmul_rn(B.diag[row], z), zf);
         B.tA[row] = t;
         acc[1] += (double)sv * (double)t;
         acc[2] += (double)t * (double)t;
@@ -1140,8 +1215,8 @@ static __global__ void __launch_bounds__(NT) k_bicg_e(BicgBufs B, InnerState* st
 // ------------------------------------------------------------ test operators
 
 // y = A x (FP32) with dot = w.y (ldu_spmv_dotw semantics, FP64 partials).
-template <int MAXW>
-static __global__ void __launch_bounds__(NT) k_spmv32(DevSell A, const float* __restrict__ diag,
+template <int MAXW, int PAIRED = 0>
+static __global__ void __launch_bounds__(NT, PAIRED ? 8 : 0) k_spmv32(DevSell A, const float* __restrict__ diag,
                                                const float* __restrict__ x,
                                                const float* __restrict__ w,
                                                float* __restrict__ y, double* out,
@@ -1150,7 +1225,7 @@ static __global__ void __launch_bounds__(NT) k_spmv32(DevSell A, const float* __
     double acc[1] = {0.0};
     CF_ROWS(row, A.n)
     {
-        const float v = row_f32<MAXW>(A, row, __fmul_rn(diag[row], x[row]),
+        const float v = row_f32<MAXW, PAIRED>(A, row, __fmul_rn(diag[row], x[row]),
                                       [&](int c) { return __ldg(x + c); });
         y[row] = v;
         if (w) acc[0] += (double)w[row] * (double)v;

@@ -69,13 +69,13 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
             }
             if (j == order - 1)
             {
-                auto fn = k_cheb_step<true, MW>;
+                auto fn = A.pval ? k_cheb_step<true, MW, 1> : k_cheb_step<true, MW, 0>;
                 fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j,
                                                                     c->d_st, c->d_part);
             }
             else
             {
-                auto fn = k_cheb_step<false, MW>;
+                auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
                 fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j,
                                                                     c->d_st, c->d_part);
             }
@@ -91,7 +91,7 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
     }
     else
     {
-        auto fn = k_pcg_p_spmv<MW>;
+        auto fn = k_pcg_p_spmv<MW, 0>;
         fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, wA, c->d_st, c->d_part);
         CF_LAUNCH();
         ++nk;
@@ -124,10 +124,10 @@ int launch_bicg_body(cf_context* c, cudaGraphConditionalHandle h, int useCond, i
     }
     else
     {
-        auto fab = k_bicg_ab<MW>;
+        auto fab = A.pval ? k_bicg_ab<MW, 1> : k_bicg_ab<MW, 0>;
         fab<<<grid_for(c, (const void*)fab, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
         CF_LAUNCH();
-        auto fcd = k_bicg_cd<MW>;
+        auto fcd = A.pval ? k_bicg_cd<MW, 1> : k_bicg_cd<MW, 0>;
         fcd<<<grid_for(c, (const void*)fcd, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part, h,
                                                               useCond);
         CF_LAUNCH();
@@ -707,8 +707,9 @@ extern "C" int cf_spmv32(cf_context* c, const float* x, const float* w, float* y
     }
     else
     {
-        auto fn = k_spmv32<MW>;
-        fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(sell_of(c), c->d_diag32, c->d_Z0,
+        const DevSell A = sell_of(c);
+        auto fn = A.pval ? k_spmv32<MW, 1> : k_spmv32<MW, 0>;
+        fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, c->d_diag32, c->d_Z0,
                                                          w ? c->d_Z1 : nullptr, c->d_W1,
                                                          c->d_scratch64, &c->d_drv->ticket,
                                                          c->d_part);
@@ -759,7 +760,7 @@ extern "C" int cf_cheb_apply(cf_context* c, const float* r, float* z, int32_t or
         }
         else
         {
-            auto fn = k_cheb_step<false, MW>;
+            auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
             fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)],
                                                              j, c->d_st, c->d_part);
             CF_LAUNCH();
@@ -812,7 +813,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
         }
         double total = 0.0;
         int rc = CF_OK;
-        auto fn = k_spmv32<MW>;
+        auto fn = A.pval ? k_spmv32<MW, 1> : k_spmv32<MW, 0>;
         const int g = grid_for(c, (const void*)fn, n);
         cudaMemsetAsync(flush, 0, flushBytes, s);
         const int gf = grid_for(c, (const void*)k_read_flush, (long long)(flushBytes / 16));
@@ -869,22 +870,24 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
                 const float* zin = (j == 1) ? B.W0 : Z[chebz(j - 1)];
                 const float* win = (j == 1) ? B.W0 : B.W1;
                 cudaEventRecord(ev[2 * k], s);
-                if (j == 7)
-                    k_cheb_step<true, MW><<<grid_for(c, (const void*)k_cheb_step<true, MW>, n), NT,
-                                            0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st,
-                                                    c->d_part);
-                else
-                    k_cheb_step<false, MW><<<grid_for(c, (const void*)k_cheb_step<false, MW>, n),
-                                             NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j,
-                                                         c->d_st, c->d_part);
+                {
+                    auto fn = j == 7 ? (A.pval ? k_cheb_step<true, MW, 1> : k_cheb_step<true, MW, 0>)
+                                     : (A.pval ? k_cheb_step<false, MW, 1>
+                                               : k_cheb_step<false, MW, 0>);
+                    fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(
+                        A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st, c->d_part);
+                }
                 cudaEventRecord(ev[2 * k + 1], s);
                 ++k;
                 const cudaError_t e = cudaGetLastError();
                 if (e != cudaSuccess) rc = fail(CF_ERR_CUDA, cudaGetErrorString(e));
             }
             if (rc != CF_OK) break;
-            k_pcg_p_spmv<MW><<<grid_for(c, (const void*)k_pcg_p_spmv<MW>, n), NT, 0, s>>>(
-                A, B, Z[chebz(7)], c->d_st, c->d_part);
+            {
+                auto fp = k_pcg_p_spmv<MW, 0>;
+                fp<<<grid_for(c, (const void*)fp, n), NT, 0, s>>>(A, B, Z[chebz(7)], c->d_st,
+                                                                 c->d_part);
+            }
             k_pcg_update<true><<<grid_for(c, (const void*)k_pcg_update<true>, n), NT, 0, s>>>(
                 B, c->d_st, c->d_part, 0, 0);
         }
@@ -923,7 +926,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             {
                 if (!spmv_default(c))
                     return launch_cheb_step_v(c, false, B, B.Z0, B.W1, B.W1, B.Z1, 2);
-                auto fn = k_cheb_step<false, MW>;
+                auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2,
                                                                  c->d_st, c->d_part);
                 break;
@@ -932,7 +935,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             {
                 if (!spmv_default(c))
                     return launch_spmv32_v(c, B.diag, B.Z0, B.W0, B.Z1, c->d_scratch64);
-                auto fn = k_spmv32<MW>;
+                auto fn = A.pval ? k_spmv32<MW, 1> : k_spmv32<MW, 0>;
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B.diag, B.Z0, B.W0, B.Z1,
                                                                  c->d_scratch64,
                                                                  &c->d_drv->ticket, c->d_part);
@@ -941,7 +944,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             case CF_KERNEL_PCG_P_SPMV:
             {
                 if (!spmv_default(c)) return launch_pcg_p_spmv_v(c, B, B.Z0);
-                auto fn = k_pcg_p_spmv<MW>;
+                auto fn = k_pcg_p_spmv<MW, 0>;
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, c->d_st, c->d_part);
                 break;
             }
