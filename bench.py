@@ -563,9 +563,12 @@ def run_gamg(ctx, d_diag, d_upper, d_src, stream, ms_reference, steps=5):
 
 def run_multi_rhs(local, stream, steps=3, dims=(64, 64, 64)):
     """One 64^3 upwind momentum matrix with 3 right-hand sides (Ux, Uy, Uz):
-    cf_solve_multi (matrix read once per SpMV for all components) vs three
-    cf_solve calls in sequence, inputs resident, same options (tolerance
-    1e-6); results are identical bit for bit (checked in the tests)."""
+    cf_solve_multi in its default form (the components as concurrent single
+    solves sharing the matrix) and in its fused form (rhsTile 4: every SpMV
+    reads the matrix once for all components) vs three cf_solve calls in
+    sequence and vs cf_solve_many_device over one context per component,
+    inputs resident, same options (tolerance 1e-6); results are identical
+    bit for bit (checked in the tests)."""
     import torch
 
     from metal4foam_b200 import _lib, mesh
@@ -583,10 +586,13 @@ def run_multi_rhs(local, stream, steps=3, dims=(64, 64, 64)):
     o = _lib.default_options(tolerance=1e-6, maxIter=1000)
     res = {}
 
-    def multi():
+    def multi(key="m"):
         d_x.zero_()
         ctx.set_coeffs_device(d_diag, d_up, d_lo)
-        res["m"] = ctx.solve_multi_device(_lib.CF_SOLVER_PBICGSTAB, d_x, d_b, o)
+        res[key] = ctx.solve_multi_device(_lib.CF_SOLVER_PBICGSTAB, d_x, d_b, o)
+
+    def fused():
+        multi("f")
 
     def single():
         d_x.zero_()
@@ -617,6 +623,9 @@ def run_multi_rhs(local, stream, steps=3, dims=(64, 64, 64)):
     ms_m = time_cuda(multi, steps, stream) / steps
     ms_s = time_cuda(single, steps, stream) / steps
     ms_c = time_cuda(concurrent, steps, stream) / steps
+    ctx.set_spmv_config(rhsTile=4)
+    fused()
+    ms_f = time_cuda(fused, steps, stream) / steps
     ctx.close()
     for c in cs:
         c.close()
@@ -625,6 +634,12 @@ def run_multi_rhs(local, stream, steps=3, dims=(64, 64, 64)):
                         "cudaPBiCGStab, tolerance 1e-6",
             "multi_ms": round(ms_m, 3), "sequential_single_ms": round(ms_s, 3),
             "speedup": round(ms_s / ms_m, 3),
+            "multi_form": "rhsTile 0: concurrent single solves sharing one matrix copy",
+            "fused_ms": round(ms_f, 3),
+            "fused_note": "rhsTile 4: fused passes, every SpMV reading the matrix once for "
+                          "all components",
+            "iterations_equal_fused": [p.nIterations for p in res["f"]] ==
+                                      [p.nIterations for p in res["s"]],
             "component_solves_per_s": round(R / (ms_m / 1e3), 2),
             "iterations": [p.nIterations for p in res["m"]],
             "iterations_equal_single": [p.nIterations for p in res["m"]] ==

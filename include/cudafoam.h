@@ -347,10 +347,16 @@ int cf_batch_solve_device(cf_batch* batch, int32_t solver, double* const* psi,
  * component).  cf_solve_multi solves nrhs systems A psi_k = source_k on the
  * matrix of the last cf_set_coeffs together: psi and source hold nrhs
  * component fields of nCells each (component k at offset k*nCells), perf
- * has nrhs entries.  Every SpMV reads the matrix once for up to 4
- * components; each component keeps its own scalars, early exit, stopping
- * tests and restarts, and its results equal those of cf_solve on that
- * component alone.  solver must be CF_SOLVER_PBICGSTAB (momentum).
+ * has nrhs entries.  Two forms, chosen by the context's rhsTile
+ * (cf_set_spmv_config):
+ *   rhsTile 0 (default): the components run at once as single solves, up
+ *     to 8 side by side, each on its own stream and host thread, with the
+ *     matrix stored once (the context's arrays, read by all);
+ *   rhsTile 1..4: fused passes in which every SpMV reads the matrix once
+ *     for up to rhsTile components.
+ * In both, each component keeps its own scalars, early exit, stopping tests
+ * and restarts, and its results equal those of cf_solve on that component
+ * alone, bit for bit.  solver must be CF_SOLVER_PBICGSTAB (momentum).
  * cf_residual keeps referring to the last single solve. */
 int cf_solve_multi(cf_context* ctx, int32_t solver, int32_t nrhs, double* psi,
                    const double* source, const cf_options* opts,
@@ -489,14 +495,17 @@ int cf_inner_step(cf_context* ctx, int32_t step, cf_step_io* io);
  *     ranges of losortAddr -> lowerAddr / lower, metalFoamKernels.metal:64-109),
  *     rowsPerWarp 32 (row per thread), 8, 4 or 1 (warp per row: the lanes
  *     of a row load its entries and form the products together);
- *   blockSize 128, 256 or 512 threads; rhsTile 1..4 components per pass of
- *   cf_solve_multi.
+ *   blockSize 128, 256 or 512 threads; rhsTile 1..4 components per fused
+ *   pass of cf_solve_multi, or 0 for its concurrent form (components as
+ *   single solves side by side).
  * Every shape forms each row of A x with the same operations in the same
  * order (the products of a row are added one by one in the reference's
  * entry order), so A x is bit-identical across shapes; dot products fold
  * their partial sums in a shape-dependent order.  The default is SELL32,
- * 32 rows per warp, 256 threads, rhsTile 4, indexBits 16.  The batched kernels
- * (cf_batch_*) and the multi-RHS kernels always use the default shape. */
+ * 32 rows per warp, 256 threads, rhsTile 0, indexBits 16.  cf_autotune times
+ * the layouts and, when rhsTile is 1..4, the fused tile; it keeps rhsTile 0.
+ * The batched kernels (cf_batch_*) and the fused multi-RHS kernels always use
+ * the default layout; the concurrent multi-RHS form uses the context's. */
 enum
 {
     CF_LAYOUT_SELL32 = 0,

@@ -127,7 +127,7 @@ LAYOUTS = {"sell32": CF_LAYOUT_SELL32, "ldu": CF_LAYOUT_LDU}
 LAYOUT_NAMES = {v: k for k, v in LAYOUTS.items()}
 
 
-def spmv_config(layout="sell32", rowsPerWarp=32, blockSize=256, rhsTile=4, indexBits=16):
+def spmv_config(layout="sell32", rowsPerWarp=32, blockSize=256, rhsTile=0, indexBits=16):
     return SpmvConfig(LAYOUTS[layout] if isinstance(layout, str) else int(layout),
                       int(rowsPerWarp), int(blockSize), int(rhsTile), int(indexBits))
 

@@ -967,8 +967,8 @@ int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int
     for (int j = 1; j < degree; ++j)
     {
         auto fn = k_cheb_step<false, MW>;
-        fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, xa, j == 1 ? B.W0 : B.W1, B.W1,
-                                                            Z[zi], j, c->d_st, c->d_part);
+        fn<<<rows_grid(c->n), NT, 0, s>>>(A, B, xa, j == 1 ? B.W0 : B.W1, B.W1, Z[zi], j, c->d_st,
+                                          c->d_part);
         AMG_LAUNCH();
         xa = Z[zi];
         zi ^= 1;
@@ -1002,8 +1002,7 @@ int launch_amg_body(cf_context* c, int degree, cudaGraphConditionalHandle h, int
         else
         {
             auto fn = k_cheb_step<false, MW>;
-            fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, xin, B.W1, B.W1, xout, j,
-                                                                c->d_st, c->d_part);
+            fn<<<rows_grid(c->n), NT, 0, s>>>(A, B, xin, B.W1, B.W1, xout, j, c->d_st, c->d_part);
         }
         AMG_LAUNCH();
         std::swap(xin, xout);

@@ -155,8 +155,8 @@ extern "C" int cf_inner_step(cf_context* c, int32_t step, cf_step_io* io)
             else
             {
                 auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
-                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W0, B.W1, B.Z1,
-                                                                 io->chebStep, c->d_st, c->d_part);
+                fn<<<rows_grid(n), NT, 0, s>>>(A, B, B.Z0, B.W0, B.W1, B.Z1, io->chebStep,
+                                               c->d_st, c->d_part);
                 CF_LAUNCH();
             }
             CF_TRY(get(c, B.W1, io->wOut));

@@ -83,6 +83,8 @@ int dalloc(cf_context* c, T** p, size_t count)
 
 void free_topology(cf_context* c)
 {
+    for (cf_context* k : c->clones) cf_context_destroy(k);
+    c->clones.clear();
     cf_multi_release(c);
     amg_release(c);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
@@ -787,6 +789,108 @@ int stage_coeffs_from_device(cf_context* c)
     CF_TRY(stage_diag32(c, 0));
     c->hasCoeffs = true;
     return CF_OK;
+}
+
+}  // namespace cf
+
+namespace cf {
+
+int context_clone_matrix(cf_context* src, cf_context** out)
+{
+    *out = nullptr;
+    cf_context* c = nullptr;
+    CF_TRY(cf_context_create(&c, src->device));
+    struct Guard
+    {
+        cf_context* c;
+        ~Guard()
+        {
+            if (c) cf_context_destroy(c);
+        }
+    } guard{c};
+    c->reorderMode = src->reorderMode;
+    c->topoReorderMode = src->topoReorderMode;
+    c->n = src->n;
+    c->nf = src->nf;
+    c->nslices = src->nslices;
+    c->nnzp = src->nnzp;
+    c->maxRowLen = src->maxRowLen;
+    c->ellW = src->ellW;
+    c->perm = src->perm;
+    c->identityPerm = src->identityPerm;
+    c->clusterShift = src->clusterShift;
+    c->clusterRemote = src->clusterRemote;
+    // vectors of its own (the FP32 diagonal included: every solve stages it)
+    const size_t N = (size_t)src->n;
+    const int nf = src->nf;
+    CF_TRY(dalloc(c, &c->d_diag32, N));
+    CF_TRY(dalloc(c, &c->d_rD32, N));
+    CF_TRY(dalloc(c, &c->d_psi, N));
+    CF_TRY(dalloc(c, &c->d_b, N));
+    CF_TRY(dalloc(c, &c->d_r64, N));
+    CF_TRY(dalloc(c, &c->d_io64, N));
+    CF_TRY(dalloc(c, &c->d_io64b, N));
+    CF_TRY(dalloc(c, &c->d_r0, N));
+    CF_TRY(dalloc(c, &c->d_gU, (size_t)std::max(nf, 1)));
+    CF_TRY(dalloc(c, &c->d_gL, (size_t)std::max(nf, 1)));
+    CF_TRY(dalloc(c, &c->d_gD, N));
+    CF_TRY(dalloc(c, &c->d_rA, N));
+    CF_TRY(dalloc(c, &c->d_W0, N));
+    CF_TRY(dalloc(c, &c->d_W1, N));
+    CF_TRY(dalloc(c, &c->d_Z0, N));
+    CF_TRY(dalloc(c, &c->d_Z1, N));
+    CF_TRY(dalloc(c, &c->d_P, 2 * N));
+    CF_TRY(dalloc(c, &c->d_Q, 2 * N));
+    CF_TRY(dalloc(c, &c->d_T, N));
+    CF_TRY(dalloc(c, &c->d_D, 3 * N));
+    CF_TRY(dalloc(c, &c->d_io32, N));
+    CF_TRY(dalloc(c, &c->d_io32b, N));
+    CF_TRY(dalloc(c, &c->d_io32c, N));
+    CF_CUDA(cudaMemsetAsync(c->d_D, 0, sizeof(float) * 3 * N, c->stream));
+    CF_CUDA(cudaMemsetAsync(c->d_r64, 0, sizeof(double) * N, c->stream));
+    CF_CUDA(cudaStreamSynchronize(c->stream));
+    c->hasTopo = true;
+    c->hasCoeffs = true;
+    CF_TRY(context_clone_sync(src, c));
+    guard.c = nullptr;
+    *out = c;
+    return CF_OK;
+}
+
+int context_clone_sync(cf_context* src, cf_context* c)
+{
+    // the matrix: src's arrays, read only (they stay in src's allocations)
+    c->d_sliceOff = src->d_sliceOff;
+    c->d_col = src->d_col;
+    c->d_col16 = src->d_col16;
+    c->d_pcol16 = src->d_pcol16;
+    c->d_eface = src->d_eface;
+    c->d_perm = src->d_perm;
+    c->d_low = src->d_low;
+    c->d_upp = src->d_upp;
+    c->d_val32 = src->d_val32;
+    c->d_pval32 = src->d_pval32;
+    c->d_val64 = src->d_val64;
+    c->d_valT64 = src->d_valT64;
+    c->d_diagIn = src->d_diagIn;
+    c->d_upper = src->d_upper;
+    c->d_lower = src->d_lower;
+    c->d_diag64 = src->d_diag64;
+    c->d_u = src->d_u;
+    c->lduReady = src->lduReady;
+    c->d_own = src->d_own;
+    c->d_losS = src->d_losS;
+    c->d_los = src->d_los;
+    c->d_uppI = src->d_uppI;
+    c->d_lowI = src->d_lowI;
+    c->d_face32 = src->d_face32;
+    c->hasLower = src->hasLower;
+    c->val32Sym = src->val32Sym;
+    c->transposed = src->transposed;
+    c->waitPolls = src->waitPolls;
+    cf_spmv_config k;
+    CF_TRY(cf_get_spmv_config(src, &k));
+    return cf_set_spmv_config(c, &k);
 }
 
 }  // namespace cf

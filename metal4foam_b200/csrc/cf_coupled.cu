@@ -963,8 +963,8 @@ int inner_solve(Ctx& x, bool bicg, const double* mean, double target, int maxIte
                     else
                     {
                         auto fn = k_cheb_step<false, MW>;
-                        fn<<<grid_of(d, (const void*)fn, n), NT, 0, s>>>(
-                            A, B, zin, win, B.W1, Z[j & 1], j, d->d_st, d->d_part);
+                        fn<<<rows_grid(n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[j & 1], j,
+                                                       d->d_st, d->d_part);
                         CF_LAUNCH();
                     }
                 }

@@ -108,6 +108,7 @@ struct cf_context
 
     // several right-hand sides on this matrix (cf_multi.cu), built on first use
     void* multi = nullptr;
+    std::vector<cf_context*> clones;       // contexts solving on this matrix (multi-RHS streams)
 
     // SpMV launch shape of the FP32 Krylov kernels (cf_tune.cu): layout
     // (CF_LAYOUT_*), rows per warp, block size, multi-RHS tile
@@ -122,7 +123,7 @@ struct cf_context
     int cfgLayout = 0;
     int cfgRowsPerWarp = 32;
     int cfgBlockSize = 256;
-    int cfgRhsTile = 4;
+    int cfgRhsTile = 0;         // 0: multi-RHS components as concurrent single solves
     int cfgIndexBits = 16;      // SELL-32 column stream: 16 (when built) or 32
     // the reference's addressing read directly (CF_LAYOUT_LDU), built on
     // first use; topology-lifetime allocations
@@ -137,6 +138,16 @@ struct cf_context
 
 // Frees the multi-RHS buffers and graphs (with the topology they point into).
 void cf_multi_release(cf_context* c);
+
+namespace cf {
+// A context that solves on src's matrix: src's topology and coefficient
+// arrays (read only, shared), every vector, state, graph and the FP32
+// diagonal its own.  Freed with src's topology.
+int context_clone_matrix(cf_context* src, cf_context** out);
+// Refreshes a clone's own copies (FP32 diagonal, staging flags, launch
+// shape) from src before a solve on src's current coefficients.
+int context_clone_sync(cf_context* src, cf_context* clone);
+}  // namespace cf
 
 namespace cf {
 
@@ -166,6 +177,10 @@ int build_layout(int32_t n, int32_t nf, const int32_t* low, const int32_t* upp,
 int fail(int code, const std::string& msg);
 double wall_now();
 int grid_for(cf_context* c, const void* fn, long long work);
+// One thread per row: the grid of row kernels without a grid-wide sum (their
+// results do not depend on the grid; blocks that retire early are replaced,
+// which keeps more loads in flight than a grid-stride loop per thread).
+inline int rows_grid(long long n) { return (int)std::max(1LL, (n + NT - 1) / NT); }
 DevSell sell_of(const cf_context* c);
 PcgBufs pcg_bufs(const cf_context* c);
 BicgBufs bicg_bufs(const cf_context* c);

@@ -834,8 +834,12 @@ static __global__ void __launch_bounds__(NT) k_pcg_init(PcgBufs B, const double*
 // encoded per step at metalFoamBackend.C:365-384) fused into one pass:
 //   v = A z_{j-1};  w = c2 w + c3 rD (r - v);  z_j = z_{j-1} + w.
 // On the last step the z.r dot and reduce_scalars mode 0 (wArA, beta) follow.
+// The last step's z.r sum folds in a grid-dependent order, so it runs on the
+// occupancy grid of both streams (paired: registers capped to keep the
+// unpaired occupancy); the other steps run one row per thread with
+// registers as the compiler wants them (rows_grid).
 template <bool LAST, int MAXW, int PAIRED = 0>
-static __global__ void __launch_bounds__(NT, PAIRED ? 8 : 0) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
+static __global__ void __launch_bounds__(NT, (PAIRED && LAST) ? 8 : 0) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
                                                   const float* win, float* wout, float* zout,
                                                   int j, InnerState* st, double* part)
 {

@@ -19,6 +19,8 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 using namespace cf;
 
@@ -50,6 +52,8 @@ namespace {
 
 constexpr int MW = MAXW_UNROLL;
 constexpr int RMAX = 4;
+// components solved at once by the concurrent form (rhsTile 0)
+constexpr int MAX_STREAM_COMPONENTS = 8;
 
 struct MBufs
 {
@@ -984,6 +988,73 @@ int solve_multi_R(cf_context* c, double* psi, const double* src, cudaMemcpyKind 
     return CF_OK;
 }
 
+// rhsTile 0: the components as single solves, all at once, each on a
+// context of its own (cf::context_clone_matrix: this context's matrix arrays,
+// its own vectors, stream and captured loops) driven from a host thread of
+// its own.  Every component gets exactly what cf_solve returns for it alone.
+// Solves of one component are a chain of short kernels and host
+// synchronisations that leave most of the GPU idle on meshes below a few
+// million cells; the concurrent chains fill it, and the matrix is stored once.
+int solve_multi_streams(cf_context* c, int32_t solver, int32_t nrhs, double* psi,
+                        const double* src, cudaMemcpyKind kind, const cf_options* o,
+                        cf_performance* perf)
+{
+    const size_t n = (size_t)c->n;
+    const int W = std::min<int>(nrhs, MAX_STREAM_COMPONENTS);
+    while ((int)c->clones.size() < W)
+    {
+        cf_context* k = nullptr;
+        CF_TRY(context_clone_matrix(c, &k));
+        c->clones.push_back(k);
+    }
+    // the FP32 operator in BiCGStab's form, staged once on the shared arrays
+    const int wantSym32 = c->hasLower ? 0 : 1;
+    if (wantSym32 != c->val32Sym) CF_TRY(stage_vals(c, wantSym32));
+    for (int w = 0; w < W; ++w) CF_TRY(context_clone_sync(c, c->clones[w]));
+    // the clones' streams start after the work queued so far on this one
+    CF_CUDA(cudaEventRecord(c->ev0, c->stream));
+    for (int w = 0; w < W; ++w) CF_CUDA(cudaStreamWaitEvent(c->clones[w]->stream, c->ev0, 0));
+    std::vector<int> rc(nrhs, CF_OK);
+    std::vector<std::string> msg(nrhs);
+    auto run = [&](int w) {
+        for (int k = w; k < nrhs; k += W)
+        {
+            double* p = psi + k * n;
+            const double* b = src + k * n;
+            const int r = kind == cudaMemcpyHostToDevice
+                              ? cf_solve(c->clones[w], solver, p, b, o, &perf[k])
+                              : cf_solve_device(c->clones[w], solver, p, b, o, &perf[k]);
+            if (r != CF_OK)
+            {
+                rc[k] = r;
+                msg[k] = cf_last_error();
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    std::vector<int> inlineRuns;
+    for (int w = 1; w < W; ++w)
+    {
+        try
+        {
+            pool.emplace_back(run, w);
+        }
+        catch (...)
+        {
+            inlineRuns.push_back(w);   // no exception crosses the C ABI
+        }
+    }
+    run(0);
+    for (int w : inlineRuns) run(w);
+    for (auto& t : pool) t.join();
+    for (int k = 0; k < nrhs; ++k)
+        if (rc[k] != CF_OK) return fail(rc[k], "component " + std::to_string(k) + ": " + msg[k]);
+    for (int w = 0; w < W; ++w)
+        c->launches += c->clones[w]->launches, c->clones[w]->launches = 0;
+    return CF_OK;
+}
+
 int solve_multi(cf_context* c, int32_t solver, int32_t nrhs, double* psi, const double* src,
                 cudaMemcpyKind kind, const cf_options* o, cf_performance* perf)
 {
@@ -999,6 +1070,7 @@ int solve_multi(cf_context* c, int32_t solver, int32_t nrhs, double* psi, const 
     if (nrhs < 1) return fail(CF_ERR_INVALID_ARG, "nrhs must be >= 1");
     CF_CUDA(cudaSetDevice(c->device));
     if (c->transposed) return fail(CF_ERR_UNSUPPORTED, "transposed operator staged");
+    if (c->cfgRhsTile == 0) return solve_multi_streams(c, solver, nrhs, psi, src, kind, o, perf);
     const size_t n = (size_t)c->n;
     // components per pass: the context's RHS tile (cf_set_spmv_config / cf_autotune)
     const int tile = std::max(1, std::min(RMAX, c->cfgRhsTile));

@@ -76,8 +76,8 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
             else
             {
                 auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
-                fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j,
-                                                                    c->d_st, c->d_part);
+                fn<<<rows_grid(c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j, c->d_st,
+                                                  c->d_part);
             }
             CF_LAUNCH();
             ++nk;
@@ -761,8 +761,8 @@ extern "C" int cf_cheb_apply(cf_context* c, const float* r, float* z, int32_t or
         else
         {
             auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
-            fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)],
-                                                             j, c->d_st, c->d_part);
+            fn<<<rows_grid(n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st,
+                                           c->d_part);
             CF_LAUNCH();
         }
         out = Z[chebz(j)];
@@ -874,7 +874,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
                     auto fn = j == 7 ? (A.pval ? k_cheb_step<true, MW, 1> : k_cheb_step<true, MW, 0>)
                                      : (A.pval ? k_cheb_step<false, MW, 1>
                                                : k_cheb_step<false, MW, 0>);
-                    fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(
+                    fn<<<j == 7 ? grid_for(c, (const void*)fn, n) : rows_grid(n), NT, 0, s>>>(
                         A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st, c->d_part);
                 }
                 cudaEventRecord(ev[2 * k + 1], s);
@@ -927,8 +927,8 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
                 if (!spmv_default(c))
                     return launch_cheb_step_v(c, false, B, B.Z0, B.W1, B.W1, B.Z1, 2);
                 auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
-                fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2,
-                                                                 c->d_st, c->d_part);
+                fn<<<rows_grid(n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2, c->d_st,
+                                               c->d_part);
                 break;
             }
             case CF_KERNEL_SPMV32:

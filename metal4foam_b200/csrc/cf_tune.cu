@@ -564,7 +564,7 @@ bool valid_config(const cf_spmv_config& k)
 {
     if (k.indexBits != 16 && k.indexBits != 32) return false;
     if (k.blockSize != 128 && k.blockSize != 256 && k.blockSize != 512) return false;
-    if (k.rhsTile < 1 || k.rhsTile > 4) return false;
+    if (k.rhsTile < 0 || k.rhsTile > 4) return false;
     if (k.layout == CF_LAYOUT_SELL32) return k.rowsPerWarp == 32;
     if (k.layout == CF_LAYOUT_LDU)
         return k.rowsPerWarp == 32 || k.rowsPerWarp == 8 || k.rowsPerWarp == 4 ||
@@ -788,7 +788,7 @@ extern "C" int cf_spmv_config_default(cf_spmv_config* k)
     k->layout = CF_LAYOUT_SELL32;
     k->rowsPerWarp = 32;
     k->blockSize = NT;
-    k->rhsTile = 4;
+    k->rhsTile = 0;
     k->indexBits = 16;
     return CF_OK;
 }
@@ -807,7 +807,7 @@ extern "C" int cf_set_spmv_config(cf_context* c, const cf_spmv_config* k)
     if (!valid_config(*k))
         return fail(CF_ERR_UNSUPPORTED,
                     "SpMV configuration not offered (layout SELL32: rowsPerWarp 32; layout LDU: "
-                    "rowsPerWarp 32, 8, 4 or 1; blockSize 128, 256 or 512; rhsTile 1..4; "
+                    "rowsPerWarp 32, 8, 4 or 1; blockSize 128, 256 or 512; rhsTile 0..4; "
                     "indexBits 16 or 32)");
     if (k->layout == CF_LAYOUT_LDU)
     {
@@ -879,7 +879,18 @@ extern "C" int cf_autotune(cf_context* c, int32_t reps, int32_t apply, cf_spmv_c
     apply_config(c, saved);
     if (rc != CF_OK) return rc;
 
-    // RHS tile: least time per component of the multi-component SpMV
+    // RHS tile of the fused multi-RHS form: least time per component of the
+    // multi-component SpMV.  The concurrent form (rhsTile 0, whole solves
+    // side by side) is kept: an SpMV timing cannot rank it against the fused
+    // passes.
+    if (saved.rhsTile == 0)
+    {
+        win.rhsTile = 0;
+        *best = win;
+        if (count) *count = nt;
+        if (apply) apply_config(c, win);
+        return CF_OK;
+    }
     float* xm = nullptr;
     float* ym = nullptr;
     if (cudaMalloc((void**)&xm, sizeof(float) * 4 * (size_t)n) != cudaSuccess ||

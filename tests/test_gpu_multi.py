@@ -1,8 +1,10 @@
 """Several right-hand sides on one matrix (the momentum components Ux, Uy,
 Uz of one fvMatrix): cf_solve_multi must return, per component, exactly
 what cf_solve returns for that component alone -- the same psi bit for bit,
-the same iteration and restart counts and residuals -- while every SpMV reads
-the matrix once for all components."""
+the same iteration and restart counts and residuals -- in both of its forms:
+rhsTile 0 (components as concurrent single solves sharing the matrix) and
+rhsTile 1..4 (fused passes, every SpMV reading the matrix once for all
+components of a pass)."""
 import numpy as np
 import pytest
 
@@ -13,11 +15,16 @@ pytestmark = pytest.mark.gpu
 BICG = _lib.CF_SOLVER_PBICGSTAB
 
 
-def make_ctx(s):
+FORMS = [0, 4]   # rhsTile: concurrent single solves, fused passes of 4
+
+
+def make_ctx(s, tile=0):
     ctx = _lib.Context(0)
     a = s.addr
     ctx.set_topology(a.n, a.nf, *a.arrays())
     ctx.set_coeffs(s.diag, s.upper, s.lower)
+    if tile:
+        ctx.set_spmv_config(rhsTile=tile)
     return ctx
 
 
@@ -43,11 +50,12 @@ def rhs_set(s, nrhs, seed):
     return np.ascontiguousarray(b)
 
 
-@pytest.mark.parametrize("nrhs", [1, 2, 3, 4, 5])
-def test_multi_equals_single_asymmetric(require_gpu, nrhs):
+@pytest.mark.parametrize("tile", FORMS)
+@pytest.mark.parametrize("nrhs", [1, 2, 3, 4, 5, 9])
+def test_multi_equals_single_asymmetric(require_gpu, nrhs, tile):
     s = mesh.upwind3d((20, 18, 16), seed=11)
     opts = _lib.default_options(tolerance=1e-8, maxIter=2000)
-    ctx = make_ctx(s)
+    ctx = make_ctx(s, tile)
     b = rhs_set(s, nrhs, 5)
     psi = np.zeros((nrhs, s.n))
     perfs = ctx.solve_multi(BICG, psi, b, opts)
@@ -59,10 +67,11 @@ def test_multi_equals_single_asymmetric(require_gpu, nrhs):
     ctx.close()
 
 
-def test_multi_equals_single_symmetric_permuted(require_gpu):
+@pytest.mark.parametrize("tile", FORMS)
+def test_multi_equals_single_symmetric_permuted(require_gpu, tile):
     s = mesh.varcoeff3d((14, 13, 12), seed=12, permute=True)
     opts = _lib.default_options(tolerance=1e-7, maxIter=3000)
-    ctx = make_ctx(s)
+    ctx = make_ctx(s, tile)
     b = rhs_set(s, 3, 6)
     psi0 = np.random.default_rng(7).standard_normal((3, s.n))
     psi = psi0.copy()
@@ -74,11 +83,12 @@ def test_multi_equals_single_symmetric_permuted(require_gpu):
     ctx.close()
 
 
-def test_multi_uneven_components_graph_and_host_sync(require_gpu, oracle):
+@pytest.mark.parametrize("tile", FORMS)
+def test_multi_uneven_components_graph_and_host_sync(require_gpu, oracle, tile):
     """Components that need very different work: one already solved, one
     easy, one hard; graph and host-synchronised loops agree bit for bit."""
     s = mesh.upwind3d((16, 15, 14), seed=13)
-    ctx = make_ctx(s)
+    ctx = make_ctx(s, tile)
     tight = _lib.default_options(tolerance=1e-13, relTol=0.0, maxIter=5000)
     x0 = np.zeros(s.n)
     ctx.solve(BICG, x0, s.source, tight)
@@ -101,9 +111,10 @@ def test_multi_uneven_components_graph_and_host_sync(require_gpu, oracle):
     ctx.close()
 
 
-def test_multi_max_iter_and_min_iter(require_gpu):
+@pytest.mark.parametrize("tile", FORMS)
+def test_multi_max_iter_and_min_iter(require_gpu, tile):
     s = mesh.upwind3d((12, 11, 10), seed=14)
-    ctx = make_ctx(s)
+    ctx = make_ctx(s, tile)
     b = rhs_set(s, 3, 8)
     for kw in (dict(maxIter=0), dict(maxIter=7), dict(minIter=40, tolerance=1e-3),
                dict(maxRestarts=0, maxIter=5)):
@@ -117,10 +128,11 @@ def test_multi_max_iter_and_min_iter(require_gpu):
     ctx.close()
 
 
-def test_multi_device_pointers(require_gpu):
+@pytest.mark.parametrize("tile", FORMS)
+def test_multi_device_pointers(require_gpu, tile):
     import torch
     s = mesh.upwind3d((18, 17, 9), seed=15)
-    ctx = make_ctx(s)
+    ctx = make_ctx(s, tile)
     b = rhs_set(s, 3, 9)
     opts = _lib.default_options(tolerance=1e-8)
     psi_h = np.zeros((3, s.n))
@@ -135,13 +147,14 @@ def test_multi_device_pointers(require_gpu):
     ctx.close()
 
 
-def test_multi_topology_change_rebuilds(require_gpu):
+@pytest.mark.parametrize("tile", FORMS)
+def test_multi_topology_change_rebuilds(require_gpu, tile):
     """A new mesh with the same cell count must not reuse buffers or graphs
     that point into the old topology."""
     s1 = mesh.upwind3d((10, 10, 10), seed=16)
     s2 = mesh.upwind3d((20, 10, 5), seed=17)
     assert s1.n == s2.n
-    ctx = make_ctx(s1)
+    ctx = make_ctx(s1, tile)
     opts = _lib.default_options(tolerance=1e-8)
     b = rhs_set(s1, 2, 10)
     ctx.solve_multi(BICG, np.zeros((2, s1.n)), b, opts)
@@ -156,6 +169,34 @@ def test_multi_topology_change_rebuilds(require_gpu):
         r = b2[k] - mesh.amul_numpy(s2, psi[k])
         assert np.sum(np.abs(r)) / perfs[k].normFactor == pytest.approx(perfs[k].finalResidual,
                                                                          rel=1e-9)
+    ctx.close()
+
+
+def test_concurrent_form_follows_coeffs_and_shape(require_gpu):
+    """The concurrent form solves on the context's current matrix: new
+    coefficients, the LDU layout and a symmetric matrix after an asymmetric
+    one all reach every component."""
+    s = mesh.upwind3d((15, 14, 13), seed=18)
+    ctx = make_ctx(s)
+    opts = _lib.default_options(tolerance=1e-8, maxIter=2000)
+    b = rhs_set(s, 3, 13)
+
+    def check():
+        psi = np.zeros((3, s.n))
+        perfs = ctx.solve_multi(BICG, psi, b, opts)
+        for k in range(3):
+            x1, p1 = single(ctx, np.zeros(s.n), b[k], opts)
+            assert_same(perfs[k], p1, k)
+            assert np.array_equal(psi[k], x1), k
+
+    check()
+    ctx.set_coeffs(1.5 * s.diag, 0.9 * s.upper, 1.1 * s.lower)
+    check()
+    ctx.set_spmv_config(layout="ldu", rowsPerWarp=8, blockSize=128)
+    check()
+    ctx.set_spmv_config()
+    ctx.set_coeffs(s.diag, s.upper, None)
+    check()
     ctx.close()
 
 

@@ -124,11 +124,21 @@ def test_autotune_picks_a_timed_shape(require_gpu):
     b = best.as_dict()
     keys = ("layout", "rowsPerWarp", "blockSize", "indexBits")
     assert {k: b[k] for k in keys} == {k: fastest[k] for k in keys}
-    assert 1 <= b["rhsTile"] <= 4
+    assert b["rhsTile"] == 0   # the concurrent multi-RHS form is kept
     assert ctx.spmv_config().as_dict() == b
     x = np.zeros(s.n)
     p = ctx.solve(_lib.CF_SOLVER_PCG, x, s.source, _lib.default_options())
     assert p.converged
+    ctx.close()
+
+
+def test_autotune_fused_rhs_tile(require_gpu):
+    """With the fused multi-RHS form selected, cf_autotune times the tile."""
+    s = mesh.varcoeff3d((32, 32, 32), seed=28, permute=True)
+    ctx = make_ctx(s)
+    ctx.set_spmv_config(rhsTile=4)
+    best, _ = ctx.autotune(reps=5, apply=True)
+    assert 1 <= best.as_dict()["rhsTile"] <= 4
     ctx.close()
 
 
@@ -139,7 +149,7 @@ def test_multi_rhs_tiles_bitwise(require_gpu):
     opts = _lib.default_options(tolerance=1e-8)
     ref = np.zeros((3, s.n))
     pr = ctx.solve_multi(_lib.CF_SOLVER_PBICGSTAB, ref, b, opts)
-    for tile in (1, 2):
+    for tile in (1, 2, 4):
         ctx.set_spmv_config(rhsTile=tile)
         x = np.zeros((3, s.n))
         p = ctx.solve_multi(_lib.CF_SOLVER_PBICGSTAB, x, b, opts)
