@@ -1017,8 +1017,10 @@ def profile_case(args):
     single-kernel captures), one GPU, a few GB at most:
 
       kernels  the seeded 128^3 pressure matrix (or --dims), a 2-iteration
-               solve so every work vector holds finite data, then each hot
-               kernel launched --reps times (cf_time_kernel);
+               host-synchronised solve (its Chebyshev steps are launches 0-6
+               and 7-13 of k_cheb_step, the last of each iteration with the
+               z.r sum), then each hot kernel launched --reps times
+               (cf_time_kernel);
       batched  one batched solve of the first --count (48) systems of the
                batched configuration, host-synchronised loop (graph 0: a
                profiler cannot see kernel nodes inside graphs with
@@ -1037,7 +1039,8 @@ def profile_case(args):
         ctx.set_topology(a.n, a.nf, *a.arrays())
         ctx.set_coeffs(s.diag, s.upper, None)
         psi = np.zeros(s.n)
-        ctx.solve(_lib.CF_SOLVER_PCG, psi, s.source, _lib.default_options(maxIter=2))
+        # host-synchronised: a profiler sees the iteration kernels one by one
+        ctx.solve(_lib.CF_SOLVER_PCG, psi, s.source, _lib.default_options(maxIter=2, graph=0))
         for k in ("cheb_step", "spmv32", "pcg_p_spmv", "pcg_update", "amul64"):
             print(f"{k} {ctx.time_kernel(k, reps=args.reps):.6f} ms/launch", flush=True)
         ctx.close()

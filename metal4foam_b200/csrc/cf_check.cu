@@ -147,14 +147,14 @@ extern "C" int cf_inner_step(cf_context* c, int32_t step, cf_step_io* io)
             }
             else if (last)
             {
-                auto fn = A.pval ? k_cheb_step<true, MW, 1> : k_cheb_step<true, MW, 0>;
+                auto fn = cheb_step_kernel<true>(A);
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, B.W0, B.W1, B.Z1,
                                                                  io->chebStep, c->d_st, c->d_part);
                 CF_LAUNCH();
             }
             else
             {
-                auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
+                auto fn = cheb_step_kernel<false>(A);
                 fn<<<rows_grid(n), NT, 0, s>>>(A, B, B.Z0, B.W0, B.W1, B.Z1, io->chebStep,
                                                c->d_st, c->d_part);
                 CF_LAUNCH();
@@ -215,7 +215,7 @@ extern "C" int cf_inner_step(cf_context* c, int32_t step, cf_step_io* io)
             }
             else
             {
-                auto fn = A.pval ? k_bicg_ab<MW, 1> : k_bicg_ab<MW, 0>;
+                auto fn = bicg_ab_kernel(A);
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, Bb, c->d_st, c->d_part);
                 CF_LAUNCH();
             }
@@ -234,7 +234,7 @@ extern "C" int cf_inner_step(cf_context* c, int32_t step, cf_step_io* io)
             }
             else
             {
-                auto fn = A.pval ? k_bicg_cd<MW, 1> : k_bicg_cd<MW, 0>;
+                auto fn = bicg_cd_kernel(A);
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, Bb, c->d_st, c->d_part, 0, 0);
                 CF_LAUNCH();
             }

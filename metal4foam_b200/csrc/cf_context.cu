@@ -682,7 +682,8 @@ extern "C" int cf_set_topology(cf_context* c, int32_t n, int32_t nf, const int32
                                     cudaMemcpyHostToDevice, c->stream));
             // the same stream in the paired order, with a paired copy of the
             // FP32 values (staged with them), when every slice has one width
-            if (L.uniformW > 0)
+            // with paired kernels
+            if (L.uniformW >= PAIR_MIN_W && L.uniformW <= PAIR_MAX_W)
             {
                 const int W = L.uniformW;
                 const long long sw = (long long)SLICE * W;

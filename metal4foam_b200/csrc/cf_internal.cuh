@@ -48,6 +48,12 @@ constexpr short COL16_PAD = -32768;
 // 8-byte value pair per lane, 256 contiguous bytes of values per warp and
 // pair), the last entry of an odd width alone.  Same entries as the
 // column-major order, read with half the load instructions.
+// The paired copy is kept for the slice widths of hexahedral (6), prismatic
+// (5) and tetrahedral / 2-D quadrilateral (4) meshes, each with kernels
+// compiled for that width.
+constexpr int PAIR_MIN_W = 4;
+constexpr int PAIR_MAX_W = 6;
+
 __host__ __device__ inline long long pair_index(long long sliceBase, int W, int k, int lane)
 {
     const int even = W & ~1;

@@ -232,72 +232,57 @@ __device__ __forceinline__ int col_index(int c) { return c & 0x7fffffff; }
 
 // One FP32 row of A x: acc (= diag*x_row) plus the entries in stored order
 // (owner side, then neighbour side), as ldu_spmv (metalFoamKernels.metal:131-147).
-// PAIRED = 1 reads the paired copy of the compact stream (A.pcol16/A.pval,
-// uniform width); PAIRED = 0 the column-major streams.  A kernel is compiled
-// for one of the two, so neither pays registers for the other.
+// PAIRED = W (PAIR_MIN_W..PAIR_MAX_W) reads the paired copy of the compact
+// stream (A.pcol16/A.pval) of a layout whose slices all have width W;
+// PAIRED = 0 the column-major streams.  A kernel is compiled for one of
+// them, so neither pays registers or branches for the other.
 template <int MAXW, int PAIRED = 0, class XF>
 __device__ __forceinline__ float row_f32(const DevSell& A, int row, float acc,
                                          XF xf)
 {
-    const int s = row >> 5;
-    const int b0 = A.ellW ? s * SLICE * A.ellW : __ldg(A.sliceOff + s);
-    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + s + 1) - b0) >> 5;
-    const int base = b0 + (row & 31);
     if constexpr (PAIRED != 0)
     {
-        // paired order (uniform width): one short2 and one float2 load per
-        // two entries; same entries, summed in the same order (entry
-        // offsets fit 32 bits: the layout is refused beyond 2^31 entries)
+        // paired order: one short2 and one float2 load per two entries (the
+        // last entry of an odd width alone); same entries, summed in the
+        // same order (offsets fit 32 bits: the layout is refused beyond
+        // 2^31 entries)
+        constexpr int W = PAIRED;
+        constexpr int EVEN = W & ~1;
+        const int sb = (row >> 5) * SLICE * W;
         const int lane = row & 31;
-        const int sb = s * SLICE * w;
-        if (w <= MAXW)
+        short o[W];
+        float v[W];
+#pragma unroll
+        for (int g = 0; g < EVEN / 2; ++g)
         {
-            short o[MAXW];
-            float v[MAXW];
-            const int even = w & ~1;
-#pragma unroll
-            for (int g = 0; g < MAXW / 2; ++g)
-            {
-                o[2 * g] = o[2 * g + 1] = COL16_PAD;
-                v[2 * g] = v[2 * g + 1] = 0.0f;
-                if (2 * g < even)
-                {
-                    const int e = sb + 64 * g + 2 * lane;
-                    const short2 oo = __ldcs(reinterpret_cast<const short2*>(A.pcol16 + e));
-                    const float2 vv = __ldcs(reinterpret_cast<const float2*>(A.pval + e));
-                    o[2 * g] = oo.x;
-                    o[2 * g + 1] = oo.y;
-                    v[2 * g] = vv.x;
-                    v[2 * g + 1] = vv.y;
-                }
-                else if (2 * g < w)
-                {
-                    const int e = sb + 32 * even + lane;   // the last entry of an odd width
-                    o[2 * g] = __ldcs(A.pcol16 + e);
-                    v[2 * g] = __ldcs(A.pval + e);
-                }
-            }
-            float x[MAXW];
-#pragma unroll
-            for (int k = 0; k < MAXW; ++k) x[k] = (o[k] != COL16_PAD) ? xf(row + o[k]) : 0.0f;
-#pragma unroll
-            for (int k = 0; k < MAXW; ++k)
-                if (o[k] != COL16_PAD) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
+            const int e = sb + 64 * g + 2 * lane;
+            const short2 oo = __ldcs(reinterpret_cast<const short2*>(A.pcol16 + e));
+            const float2 vv = __ldcs(reinterpret_cast<const float2*>(A.pval + e));
+            o[2 * g] = oo.x;
+            o[2 * g + 1] = oo.y;
+            v[2 * g] = vv.x;
+            v[2 * g + 1] = vv.y;
         }
-        else
+        if constexpr (W != EVEN)
         {
-            for (int k = 0; k < w; ++k)
-            {
-                const int e = (int)pair_index(sb, w, k, lane);
-                const short o = __ldcs(A.pcol16 + e);
-                if (o != COL16_PAD)
-                    acc = __fadd_rn(acc, __fmul_rn(__ldcs(A.pval + e), xf(row + o)));
-            }
+            const int e = sb + 32 * EVEN + lane;
+            o[W - 1] = __ldcs(A.pcol16 + e);
+            v[W - 1] = __ldcs(A.pval + e);
         }
+        float x[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) x[k] = (o[k] != COL16_PAD) ? xf(row + o[k]) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if (o[k] != COL16_PAD) acc = __fadd_rn(acc, __fmul_rn(v[k], x[k]));
         return acc;
     }
     else
     {
+    const int s = row >> 5;
+    const int b0 = A.ellW ? s * SLICE * A.ellW : __ldg(A.sliceOff + s);
+    const int w = A.ellW ? A.ellW : (__ldg(A.sliceOff + s + 1) - b0) >> 5;
+    const int base = b0 + (row & 31);
     if (A.col16)
     {
         // compact index stream: same columns, same order, half the bytes
@@ -834,12 +819,10 @@ static __global__ void __launch_bounds__(NT) k_pcg_init(PcgBufs B, const double*
 // encoded per step at metalFoamBackend.C:365-384) fused into one pass:
 //   v = A z_{j-1};  w = c2 w + c3 rD (r - v);  z_j = z_{j-1} + w.
 // On the last step the z.r dot and reduce_scalars mode 0 (wArA, beta) follow.
-// The last step's z.r sum folds in a grid-dependent order, so it runs on the
-// occupancy grid of both streams (paired: registers capped to keep the
-// unpaired occupancy); the other steps run one row per thread with
-// registers as the compiler wants them (rows_grid).
+// The last step (with the z.r sum) runs on its occupancy grid, the other
+// steps one row per thread (rows_grid).
 template <bool LAST, int MAXW, int PAIRED = 0>
-static __global__ void __launch_bounds__(NT, (PAIRED && LAST) ? 8 : 0) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
+static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, const float* zin,
                                                   const float* win, float* wout, float* zout,
                                                   int j, InnerState* st, double* part)
 {
@@ -1220,7 +1203,7 @@ static __global__ void __launch_bounds__(NT) k_bicg_e(BicgBufs B, InnerState* st
 
 // y = A x (FP32) with dot = w.y (ldu_spmv_dotw semantics, FP64 partials).
 template <int MAXW, int PAIRED = 0>
-static __global__ void __launch_bounds__(NT, PAIRED ? 8 : 0) k_spmv32(DevSell A, const float* __restrict__ diag,
+static __global__ void __launch_bounds__(NT) k_spmv32(DevSell A, const float* __restrict__ diag,
                                                const float* __restrict__ x,
                                                const float* __restrict__ w,
                                                float* __restrict__ y, double* out,
@@ -1258,5 +1241,25 @@ static __global__ void k_cheb_init(int n, const float* __restrict__ r, const flo
     const float c1 = chebC[0];
     CF_ROWS(row, n) w[row] = __fmul_rn(__fmul_rn(c1, rD[row]), r[row]);
 }
+
+// ------------------------------------------------- stream dispatch (host)
+
+// The instantiation of a SpMV-carrying kernel for A: the paired stream of
+// its slice width when A has one, else the column-major streams.
+#define CF_PAIRED_KERNEL(A, KERNEL, ...)                                          \
+    ((A).pval && (A).ellW == 4   ? KERNEL<__VA_ARGS__, 4>                         \
+     : (A).pval && (A).ellW == 5 ? KERNEL<__VA_ARGS__, 5>                         \
+     : (A).pval && (A).ellW == 6 ? KERNEL<__VA_ARGS__, 6>                         \
+                                 : KERNEL<__VA_ARGS__, 0>)
+static_assert(PAIR_MIN_W == 4 && PAIR_MAX_W == 6, "CF_PAIRED_KERNEL covers widths 4..6");
+
+template <bool LAST>
+inline auto cheb_step_kernel(const DevSell& A)
+{
+    return CF_PAIRED_KERNEL(A, k_cheb_step, LAST, MAXW_UNROLL);
+}
+inline auto spmv32_kernel(const DevSell& A) { return CF_PAIRED_KERNEL(A, k_spmv32, MAXW_UNROLL); }
+inline auto bicg_ab_kernel(const DevSell& A) { return CF_PAIRED_KERNEL(A, k_bicg_ab, MAXW_UNROLL); }
+inline auto bicg_cd_kernel(const DevSell& A) { return CF_PAIRED_KERNEL(A, k_bicg_cd, MAXW_UNROLL); }
 
 }  // namespace cf

@@ -726,9 +726,10 @@ int launch_multi_body(cf_context* c, cudaGraphConditionalHandle h, int useCond)
     // separate -- recomputing them for every component at every gathered
     // column measured 9% slower at 64^3 x 3 -- and each pass runs on the
     // grid of the fused kernel that contains it, so every component's sums
-    // fold exactly as the single solve's
-    const int gab = grid_for(c, (const void*)k_bicg_ab<MW>, n);
-    const int gcd = grid_for(c, (const void*)k_bicg_cd<MW>, n);
+    // fold exactly as the single solve's (the kernels it launches for this
+    // layout's stream)
+    const int gab = grid_for(c, (const void*)bicg_ab_kernel(A), n);
+    const int gcd = grid_for(c, (const void*)bicg_cd_kernel(A), n);
     km_bicg_a<R><<<gab, NT, 0, s>>>(n, M);
     CF_LAUNCH();
     km_bicg_b<R, MW><<<gab, NT, 0, s>>>(A, M);

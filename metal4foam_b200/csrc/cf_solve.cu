@@ -69,13 +69,13 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
             }
             if (j == order - 1)
             {
-                auto fn = A.pval ? k_cheb_step<true, MW, 1> : k_cheb_step<true, MW, 0>;
+                auto fn = cheb_step_kernel<true>(A);
                 fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j,
                                                                     c->d_st, c->d_part);
             }
             else
             {
-                auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
+                auto fn = cheb_step_kernel<false>(A);
                 fn<<<rows_grid(c->n), NT, 0, s>>>(A, B, zin, win, B.W1, zout, j, c->d_st,
                                                   c->d_part);
             }
@@ -124,10 +124,10 @@ int launch_bicg_body(cf_context* c, cudaGraphConditionalHandle h, int useCond, i
     }
     else
     {
-        auto fab = A.pval ? k_bicg_ab<MW, 1> : k_bicg_ab<MW, 0>;
+        auto fab = bicg_ab_kernel(A);
         fab<<<grid_for(c, (const void*)fab, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part);
         CF_LAUNCH();
-        auto fcd = A.pval ? k_bicg_cd<MW, 1> : k_bicg_cd<MW, 0>;
+        auto fcd = bicg_cd_kernel(A);
         fcd<<<grid_for(c, (const void*)fcd, c->n), NT, 0, s>>>(A, B, c->d_st, c->d_part, h,
                                                               useCond);
         CF_LAUNCH();
@@ -708,7 +708,7 @@ extern "C" int cf_spmv32(cf_context* c, const float* x, const float* w, float* y
     else
     {
         const DevSell A = sell_of(c);
-        auto fn = A.pval ? k_spmv32<MW, 1> : k_spmv32<MW, 0>;
+        auto fn = spmv32_kernel(A);
         fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, c->d_diag32, c->d_Z0,
                                                          w ? c->d_Z1 : nullptr, c->d_W1,
                                                          c->d_scratch64, &c->d_drv->ticket,
@@ -760,7 +760,7 @@ extern "C" int cf_cheb_apply(cf_context* c, const float* r, float* z, int32_t or
         }
         else
         {
-            auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
+            auto fn = cheb_step_kernel<false>(A);
             fn<<<rows_grid(n), NT, 0, s>>>(A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st,
                                            c->d_part);
             CF_LAUNCH();
@@ -813,7 +813,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
         }
         double total = 0.0;
         int rc = CF_OK;
-        auto fn = A.pval ? k_spmv32<MW, 1> : k_spmv32<MW, 0>;
+        auto fn = spmv32_kernel(A);
         const int g = grid_for(c, (const void*)fn, n);
         cudaMemsetAsync(flush, 0, flushBytes, s);
         const int gf = grid_for(c, (const void*)k_read_flush, (long long)(flushBytes / 16));
@@ -871,9 +871,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
                 const float* win = (j == 1) ? B.W0 : B.W1;
                 cudaEventRecord(ev[2 * k], s);
                 {
-                    auto fn = j == 7 ? (A.pval ? k_cheb_step<true, MW, 1> : k_cheb_step<true, MW, 0>)
-                                     : (A.pval ? k_cheb_step<false, MW, 1>
-                                               : k_cheb_step<false, MW, 0>);
+                    auto fn = j == 7 ? cheb_step_kernel<true>(A) : cheb_step_kernel<false>(A);
                     fn<<<j == 7 ? grid_for(c, (const void*)fn, n) : rows_grid(n), NT, 0, s>>>(
                         A, B, zin, win, B.W1, Z[chebz(j)], j, c->d_st, c->d_part);
                 }
@@ -926,7 +924,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             {
                 if (!spmv_default(c))
                     return launch_cheb_step_v(c, false, B, B.Z0, B.W1, B.W1, B.Z1, 2);
-                auto fn = A.pval ? k_cheb_step<false, MW, 1> : k_cheb_step<false, MW, 0>;
+                auto fn = cheb_step_kernel<false>(A);
                 fn<<<rows_grid(n), NT, 0, s>>>(A, B, B.Z0, B.W1, B.W1, B.Z1, 2, c->d_st,
                                                c->d_part);
                 break;
@@ -935,7 +933,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             {
                 if (!spmv_default(c))
                     return launch_spmv32_v(c, B.diag, B.Z0, B.W0, B.Z1, c->d_scratch64);
-                auto fn = A.pval ? k_spmv32<MW, 1> : k_spmv32<MW, 0>;
+                auto fn = spmv32_kernel(A);
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B.diag, B.Z0, B.W0, B.Z1,
                                                                  c->d_scratch64,
                                                                  &c->d_drv->ticket, c->d_part);
