@@ -173,7 +173,7 @@ extern "C" int cf_inner_step(cf_context* c, int32_t step, cf_step_io* io)
             }
             else
             {
-                auto fn = k_pcg_p_spmv<MW, 0>;
+                auto fn = pcg_p_spmv_kernel(A);
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.W0, c->d_st, c->d_part);
                 CF_LAUNCH();
             }

@@ -118,10 +118,28 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NR], double* part,
     double acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += NT)
+    // each thread adds the partials i, i + NT, i + 2 NT, ... in that order;
+    // U of them are loaded before any is added, so their L2 round trips
+    // overlap (the order of the additions is unchanged)
+    constexpr int U = NR >= 8 ? 1 : 8 / NR;
+    const int G = (int)gridDim.x;
+    int i = threadIdx.x;
+    for (; i + (U - 1) * NT < G; i += U * NT)
+    {
+        double t[NR][U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) t[r][u] = __ldcg(part + r * G + i + u * NT);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[r] += t[r][u];
+    }
+    for (; i < G; i += NT)
     {
 #pragma unroll
-        for (int r = 0; r < NR; ++r) acc[r] += __ldcg(part + r * gridDim.x + i);
+        for (int r = 0; r < NR; ++r) acc[r] += __ldcg(part + r * G + i);
     }
     block_sum<NR>(acc);
     if (threadIdx.x == 0)
@@ -854,9 +872,7 @@ static __global__ void __launch_bounds__(NT) k_cheb_step(DevSell A, PcgBufs B, c
     }
 }
 
-// pcg_update_p fused into ldu_spmv_dotw (metalFoamKernels.metal:64-109,237-247)
-// (launched with the column-major streams: its p-update at every gathered
-// column needs more registers than the paired loads leave at full occupancy):
+// pcg_update_p fused into ldu_spmv_dotw (metalFoamKernels.metal:64-109,237-247):
 // p_new = wA + beta p_old is formed on the fly for every gathered column, so
 // p never needs its own pass; writes p_new, q = A p_new; p.q -> alpha
 // (reduce_scalars mode 1).
@@ -1259,6 +1275,10 @@ inline auto cheb_step_kernel(const DevSell& A)
     return CF_PAIRED_KERNEL(A, k_cheb_step, LAST, MAXW_UNROLL);
 }
 inline auto spmv32_kernel(const DevSell& A) { return CF_PAIRED_KERNEL(A, k_spmv32, MAXW_UNROLL); }
+inline auto pcg_p_spmv_kernel(const DevSell& A)
+{
+    return CF_PAIRED_KERNEL(A, k_pcg_p_spmv, MAXW_UNROLL);
+}
 inline auto bicg_ab_kernel(const DevSell& A) { return CF_PAIRED_KERNEL(A, k_bicg_ab, MAXW_UNROLL); }
 inline auto bicg_cd_kernel(const DevSell& A) { return CF_PAIRED_KERNEL(A, k_bicg_cd, MAXW_UNROLL); }
 

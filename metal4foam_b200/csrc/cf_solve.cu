@@ -91,7 +91,7 @@ int launch_pcg_body(cf_context* c, int order, cudaGraphConditionalHandle h, int 
     }
     else
     {
-        auto fn = k_pcg_p_spmv<MW, 0>;
+        auto fn = pcg_p_spmv_kernel(A);
         fn<<<grid_for(c, (const void*)fn, c->n), NT, 0, s>>>(A, B, wA, c->d_st, c->d_part);
         CF_LAUNCH();
         ++nk;
@@ -882,7 +882,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             }
             if (rc != CF_OK) break;
             {
-                auto fp = k_pcg_p_spmv<MW, 0>;
+                auto fp = pcg_p_spmv_kernel(A);
                 fp<<<grid_for(c, (const void*)fp, n), NT, 0, s>>>(A, B, Z[chebz(7)], c->d_st,
                                                                  c->d_part);
             }
@@ -942,7 +942,7 @@ extern "C" int cf_time_kernel(cf_context* c, int32_t which, int32_t reps, double
             case CF_KERNEL_PCG_P_SPMV:
             {
                 if (!spmv_default(c)) return launch_pcg_p_spmv_v(c, B, B.Z0);
-                auto fn = k_pcg_p_spmv<MW, 0>;
+                auto fn = pcg_p_spmv_kernel(A);
                 fn<<<grid_for(c, (const void*)fn, n), NT, 0, s>>>(A, B, B.Z0, c->d_st, c->d_part);
                 break;
             }
