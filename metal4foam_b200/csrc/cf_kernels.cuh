@@ -752,6 +752,10 @@ static __global__ void __launch_bounds__(NT) k_amul64(DevSell A, const double* _
 
 // ------------------------------------------------------------ inner solves
 
+// rows whose loads k_pcg_update issues together per thread (2 keeps it at
+// 32 registers, the occupancy and grid of one row at a time)
+constexpr int PCG_UPDATE_ROWS = 2;
+
 struct PcgBufs
 {
     float* rA;          // FP32 residual
@@ -956,7 +960,10 @@ __device__ __forceinline__ void inner_sync_point(S* st, bool checkWApA)
 // pcg_update_sol_res (metalFoamKernels.metal:251-276) + the next iteration's
 // preconditioner start: delta_next = delta + alpha p; rA -= alpha q; sum|rA|;
 // Chebyshev: w0 = c1 rD rA; Jacobi: wA = rA rD and wA.rA (beta).
-template <bool CHEB>
+// Each thread takes its rows row, row + stride, ... in that order (the fold
+// order of the sums); U of them have their five loads issued before the
+// first is updated, so a thread keeps 5 U loads in flight instead of 5.
+template <bool CHEB, int U = PCG_UPDATE_ROWS>
 static __global__ void __launch_bounds__(NT) k_pcg_update(PcgBufs B, InnerState* st, double* part,
                                                    cudaGraphConditionalHandle h, int useCond)
 {
@@ -969,23 +976,41 @@ static __global__ void __launch_bounds__(NT) k_pcg_update(PcgBufs B, InnerState*
     const float alpha = (float)st->alpha;
     const float c1 = CHEB ? B.chebC[0] : 0.0f;
     double acc[2] = {0.0, 0.0};
-    CF_ROWS(row, n)
-    {
-        Dn[row] = __fadd_rn(D[row], __fmul_rn(alpha, P[row]));
-        const float rn = __fsub_rn(B.rA[row], __fmul_rn(alpha, B.Q[row]));
+    auto one = [&](int row, float d, float p, float r, float q, float rd) {
+        Dn[row] = __fadd_rn(d, __fmul_rn(alpha, p));
+        const float rn = __fsub_rn(r, __fmul_rn(alpha, q));
         B.rA[row] = rn;
         acc[0] += (double)fabsf(rn);
         if (CHEB)
         {
-            B.W0[row] = __fmul_rn(__fmul_rn(c1, B.rD[row]), rn);
+            B.W0[row] = __fmul_rn(__fmul_rn(c1, rd), rn);
         }
         else
         {
-            const float wa = __fmul_rn(rn, B.rD[row]);
+            const float wa = __fmul_rn(rn, rd);
             B.W0[row] = wa;
             acc[1] += (double)wa * (double)rn;
         }
+    };
+    const int stride = gridDim.x * NT;
+    int row = blockIdx.x * NT + threadIdx.x;
+    for (; row + (U - 1) * stride < n; row += U * stride)
+    {
+        float d[U], p[U], r[U], q[U], rd[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int i = row + u * stride;
+            d[u] = D[i];
+            p[u] = P[i];
+            r[u] = B.rA[i];
+            q[u] = B.Q[i];
+            rd[u] = B.rD[i];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) one(row + u * stride, d[u], p[u], r[u], q[u], rd[u]);
     }
+    for (; row < n; row += stride) one(row, D[row], P[row], B.rA[row], B.Q[row], B.rD[row]);
     if (grid_sum<2>(acc, part, &st->ticket) && threadIdx.x == 0)
     {
         st->res = acc[0];
@@ -1193,15 +1218,36 @@ static __global__ void __launch_bounds__(NT) k_bicg_e(BicgBufs B, InnerState* st
         return;
     }
     const float omega = (float)st->omega;
-    CF_ROWS(row, n)
-    {
-        Dn[row] = __fadd_rn(D[row], __fadd_rn(__fmul_rn(alpha, B.yA[row]),
-                                              __fmul_rn(omega, B.zA[row])));
-        const float r = __fsub_rn(B.sA[row], __fmul_rn(omega, B.tA[row]));
+    auto one = [&](int row, float d, float y, float z, float sv, float t, float r0) {
+        Dn[row] = __fadd_rn(d, __fadd_rn(__fmul_rn(alpha, y), __fmul_rn(omega, z)));
+        const float r = __fsub_rn(sv, __fmul_rn(omega, t));
         B.rA[row] = r;
         acc[0] += (double)fabsf(r);
-        acc[1] += (double)B.rA0[row] * (double)r;
+        acc[1] += (double)r0 * (double)r;
+    };
+    // rows row, row + stride, ... in that order, the loads of two issued
+    // together (as k_pcg_update)
+    const int stride = gridDim.x * NT;
+    int row = blockIdx.x * NT + threadIdx.x;
+    for (; row + stride < n; row += 2 * stride)
+    {
+        float d[2], y[2], z[2], sv[2], t[2], r0[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+        {
+            const int i = row + u * stride;
+            d[u] = D[i];
+            y[u] = B.yA[i];
+            z[u] = B.zA[i];
+            sv[u] = B.sA[i];
+            t[u] = B.tA[i];
+            r0[u] = B.rA0[i];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) one(row + u * stride, d[u], y[u], z[u], sv[u], t[u], r0[u]);
     }
+    for (; row < n; row += stride)
+        one(row, D[row], B.yA[row], B.zA[row], B.sA[row], B.tA[row], B.rA0[row]);
     if (grid_sum<2>(acc, part, &st->ticket) && threadIdx.x == 0)
     {
         st->res = acc[0];
