@@ -1,6 +1,12 @@
 /*---------------------------------------------------------------------------*\
     cudaFoam: B200 (sm_100a) Krylov solvers for OpenFOAM lduMatrix systems
 
+    Provenance: the lduMatrix::solver boilerplate of this file (run-time
+    selection registration, constructor, solve forwarding) mirrors
+    metal4Foam's metalPBiCGStab.H, Copyright (C) 2026 metal4Foam authors,
+    SPDX-License-Identifier: GPL-3.0-or-later; this file is distributed
+    under the same licence.
+
 Class
     Foam::cudaPBiCGStab
 

@@ -1,5 +1,11 @@
 /*---------------------------------------------------------------------------*\
     cudaFoam: B200 (sm_100a) Krylov solvers for OpenFOAM lduMatrix systems
+
+    Provenance: the lduMatrix::solver boilerplate of this file (run-time
+    selection registration, constructor, solve forwarding) mirrors
+    metal4Foam's metalPCG.C, Copyright (C) 2026 metal4Foam authors,
+    SPDX-License-Identifier: GPL-3.0-or-later; this file is distributed
+    under the same licence.
 \*---------------------------------------------------------------------------*/
 
 #include "cudaPCG.H"
