@@ -80,7 +80,7 @@ def read_profile_traffic():
     p = os.path.join(ROOT, "profiles", "cheb_step_varcoeff128.txt")
     try:
         for line in open(p):
-            if line.startswith("dram_bytes_per_launch_full_size:"):
+            if line.startswith(("dram_bytes_per_launch:", "dram_bytes_per_launch_full_size:")):
                 return int(float(line.split(":", 1)[1]))
     except OSError:
         pass
