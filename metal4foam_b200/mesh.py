@@ -270,6 +270,56 @@ def varcoeff3d(dims=(128, 128, 128), seed: int = 1, permute: bool = True,
                      dict(dims=dims, seed=seed, permute=permute))
 
 
+def prism_faces(nx: int, ny: int, nz: int):
+    """Internal faces of an extruded triangulated grid in LDU order: each of
+    the nx x ny quadrilaterals of a layer is cut along its diagonal into two
+    triangles, and nz layers are stacked, so an interior cell (a triangular
+    prism) has five neighbours (three lateral, two axial).  Cell of quad
+    (i, j), triangle t (0: below the diagonal, 1: above), layer k:
+    ((k ny + j) nx + i) 2 + t."""
+    def cid(i, j, k, t):
+        return ((k * ny + j) * nx + i) * 2 + t
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    pairs = [(cid(i, j, k, 0), cid(i, j, k, 1))]               # across the diagonal
+    m = i + 1 < nx
+    pairs.append((cid(i[m], j[m], k[m], 0), cid(i[m] + 1, j[m], k[m], 1)))
+    m = j + 1 < ny
+    pairs.append((cid(i[m], j[m], k[m], 1), cid(i[m], j[m] + 1, k[m], 0)))
+    for t in (0, 1):
+        m = k + 1 < nz
+        pairs.append((cid(i[m], j[m], k[m], t), cid(i[m], j[m], k[m] + 1, t)))
+    a = np.concatenate([p[0] for p in pairs]).astype(np.int64)
+    b = np.concatenate([p[1] for p in pairs]).astype(np.int64)
+    low, upp = np.minimum(a, b), np.maximum(a, b)
+    order = np.lexsort((upp, low))
+    return low[order].astype(np.int32), upp[order].astype(np.int32)
+
+
+def prism3d(dims=(24, 24, 16), seed: int = 6, permute: bool = True) -> LduSystem:
+    """Variable-coefficient pressure matrix on triangular prisms (five
+    neighbours per interior cell, see prism_faces): coefficients, reference
+    cell and source as varcoeff3d; ``dims`` = (nx, ny, nz) quadrilaterals
+    per layer and layers, 2 nx ny nz cells."""
+    nx, ny, nz = (int(d) for d in dims)
+    n = 2 * nx * ny * nz
+    rng = np.random.default_rng(seed)
+    k = 10.0 ** rng.uniform(-2.0, 2.0, n)
+    low, upp = prism_faces(nx, ny, nz)
+    coef = _varcoeff_coeffs(low, upp, k)
+    if permute:
+        newlabel = rng.permutation(n).astype(np.int64)
+        low, upp, coef = permute_cells(newlabel, low, upp, coef)
+    addr = ldu_addressing(n, low, upp)
+    diag = -(_bincount_sum(n, addr.lowerAddr, coef) + _bincount_sum(n, addr.upperAddr, coef))
+    diag[0] *= 2.0
+    b = rng.standard_normal(n)
+    b -= b.mean()
+    name = f"prism3d_{nx}x{ny}x{nz}" + ("_perm" if permute else "")
+    return LduSystem(name, addr, diag, coef, None, b, np.zeros(n),
+                     dict(dims=(nx, ny, nz), seed=seed, permute=permute))
+
+
 def _fourier_velocity(rng, nmodes=8):
     ks = rng.integers(-3, 4, size=(nmodes, 3)).astype(np.float64)
     phases = rng.uniform(0.0, 2.0 * np.pi, nmodes)

@@ -30,6 +30,27 @@ def test_addressing_3x3_by_hand(oracle):
     assert np.array_equal(losS, a.losortStartAddr)
 
 
+def test_prism_faces_by_hand(oracle):
+    """One layer of 2 x 1 quadrilaterals cut into triangles, two layers:
+    cells ((k ny + j) nx + i) 2 + t; faces across each diagonal, between
+    neighbouring quads (right edge of t0 to the left edge of the next
+    quad's t1), and between the layers."""
+    low, upp = mesh.prism_faces(2, 1, 2)
+    pairs = sorted(zip(low.tolist(), upp.tolist()))
+    want = sorted([(0, 1), (2, 3), (4, 5), (6, 7),          # diagonals
+                   (0, 3), (4, 7),                          # quad (0,0) t0 | quad (1,0) t1
+                   (0, 4), (1, 5), (2, 6), (3, 7)])         # layer 0 | layer 1
+    assert pairs == want
+    assert list(zip(low.tolist(), upp.tolist())) == want    # already in LDU order
+    s = mesh.prism3d((9, 8, 7), seed=3)
+    a = s.addr
+    own, los, losS = oracle.build_addressing(s.n, a.lowerAddr, a.upperAddr)
+    assert np.array_equal(own, a.ownerStartAddr)
+    deg = np.bincount(a.lowerAddr, minlength=s.n) + np.bincount(a.upperAddr, minlength=s.n)
+    assert deg.max() == 5 and s.n == 2 * 9 * 8 * 7
+    assert s.nf == 9 * 8 * 7 + 8 * 8 * 7 + 9 * 7 * 7 + 2 * 9 * 8 * 6
+
+
 def test_addressing_rejects_unsorted(oracle):
     low = np.array([0, 1, 0], np.int32)
     upp = np.array([1, 2, 2], np.int32)
