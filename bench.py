@@ -301,7 +301,7 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
     o = _lib.default_options(**opts)
     res = {"b": [], "p": []}
     cur = {"bt": bt}
-    solo_min = torch.cuda.get_device_properties(dev).multi_processor_count * 2048
+    solo_min = torch.cuda.get_device_properties(dev).multi_processor_count * 768
 
     def batched():
         b = cur["bt"]
@@ -421,7 +421,7 @@ def run_batched(local, stream, ws=1, rank=0, steps=3):
             "host_sync_loop_solves_per_s": round(S / (ms_h / 1e3), 2),
             "speedup_vs_plain_loop": round(ms_p / ms_b, 3),
             "batched_note": "batched = cf_batch_solve as the library runs it: systems of at "
-                            "least numSMs x 2048 cells (%d of %d here) as single solves on "
+                            "least numSMs x 768 cells (%d of %d here) as single solves on "
                             "their own streams, concurrently with one launch per phase for "
                             "the rest" % (sum(1 for s in systems if s.n >= solo_min), S),
             "one_launch_per_phase": {

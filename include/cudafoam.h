@@ -315,12 +315,13 @@ int cf_batch_add_system(cf_batch* batch, int32_t nCells, int32_t nFaces,
                         const int32_t* lowAddr, const int32_t* uppAddr,
                         const int32_t* ownStartAddr, const int32_t* losortAddr,
                         const int32_t* losortStartAddr, int32_t* index);
-/* Systems of at least minCells cells (0, the default: as many rows as the
- * device keeps resident, numSMs x 2048; < 0: never) are solved as single
+/* Systems of at least minCells cells (0, the default: three 256-row blocks
+ * per SM, numSMs x 768, 113,664 on B200; < 0: never) are solved as single
  * solves (a context of their own, cf_solve's path and result) on their own
  * host thread and stream, concurrently with the batched launches of the
- * rest: a system that fills every SM gains nothing from sharing a launch,
- * while the small ones do.  Call before cf_batch_finalize. */
+ * rest: a system that keeps several blocks busy on every SM gains little
+ * from sharing a launch, while the small ones gain from it.  Call before
+ * cf_batch_finalize. */
 int cf_batch_set_solo_cells(cf_batch* batch, int32_t minCells);
 /* Lays all systems out on the device (reorder: CF_REORDER_*, per system). */
 int cf_batch_finalize(cf_batch* batch, int32_t reorder);

@@ -34,6 +34,8 @@ using namespace cf;
 namespace {
 
 constexpr int MW = MAXW_UNROLL;
+// default solo threshold: this many NT-row blocks per SM
+constexpr int SOLO_BLOCKS_PER_SM = 3;
 
 struct BSys
 {
@@ -1539,14 +1541,16 @@ extern "C" int cf_batch_finalize(cf_batch* bt, int32_t reorder)
     if (bt->finalized) return CF_OK;
     if (bt->sys.empty()) return fail(CF_ERR_INVALID_ARG, "batch has no systems");
     CFB_CUDA(cudaSetDevice(bt->device));
-    // systems with at least a full resident grid of rows (every SM busy on
-    // their own) become solo systems
+    // systems of at least three blocks of rows per SM become solo systems:
+    // their single solves keep the GPU busy beside the others, while the
+    // small ones run their iterations as one launch per phase for all
+    // (measured on the 48-system set: 8 solo systems from numSMs x 2048
+    // rows, 588 ms; 17-19 from 3 x 256 per SM or 100,000, 545 ms)
     {
         const long long minCells =
             bt->soloMinCells > 0 ? bt->soloMinCells
-                                 : (bt->soloMinCells == 0
-                                        ? (long long)bt->numSMs * bt->maxBlocksPerSM * NT
-                                        : (1LL << 62));
+                                 : (bt->soloMinCells == 0 ? (long long)bt->numSMs * SOLO_BLOCKS_PER_SM * NT
+                                                          : (1LL << 62));
         bt->nAll = (int)bt->sys.size();
         bt->solo.assign(bt->nAll, nullptr);
         bt->inner.assign(bt->nAll, -1);

@@ -821,9 +821,10 @@ int context_clone_matrix(cf_context* src, cf_context** out)
     c->identityPerm = src->identityPerm;
     c->clusterShift = src->clusterShift;
     c->clusterRemote = src->clusterRemote;
-    // vectors of its own (the FP32 diagonal included: every solve stages it)
+    // vectors of its own (the FP32 diagonal included: every solve stages it);
+    // only cf_solve[_device] runs on a clone, so it has no face-gradient
+    // (adjoint) or FP32 staging buffers
     const size_t N = (size_t)src->n;
-    const int nf = src->nf;
     CF_TRY(dalloc(c, &c->d_diag32, N));
     CF_TRY(dalloc(c, &c->d_rD32, N));
     CF_TRY(dalloc(c, &c->d_psi, N));
@@ -832,9 +833,6 @@ int context_clone_matrix(cf_context* src, cf_context** out)
     CF_TRY(dalloc(c, &c->d_io64, N));
     CF_TRY(dalloc(c, &c->d_io64b, N));
     CF_TRY(dalloc(c, &c->d_r0, N));
-    CF_TRY(dalloc(c, &c->d_gU, (size_t)std::max(nf, 1)));
-    CF_TRY(dalloc(c, &c->d_gL, (size_t)std::max(nf, 1)));
-    CF_TRY(dalloc(c, &c->d_gD, N));
     CF_TRY(dalloc(c, &c->d_rA, N));
     CF_TRY(dalloc(c, &c->d_W0, N));
     CF_TRY(dalloc(c, &c->d_W1, N));
@@ -844,9 +842,6 @@ int context_clone_matrix(cf_context* src, cf_context** out)
     CF_TRY(dalloc(c, &c->d_Q, 2 * N));
     CF_TRY(dalloc(c, &c->d_T, N));
     CF_TRY(dalloc(c, &c->d_D, 3 * N));
-    CF_TRY(dalloc(c, &c->d_io32, N));
-    CF_TRY(dalloc(c, &c->d_io32b, N));
-    CF_TRY(dalloc(c, &c->d_io32c, N));
     CF_CUDA(cudaMemsetAsync(c->d_D, 0, sizeof(float) * 3 * N, c->stream));
     CF_CUDA(cudaMemsetAsync(c->d_r64, 0, sizeof(double) * N, c->stream));
     CF_CUDA(cudaStreamSynchronize(c->stream));
