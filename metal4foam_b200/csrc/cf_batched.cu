@@ -479,6 +479,37 @@ __global__ void __launch_bounds__(NT) kb_cheb_step(BArgs B, const float* zin, co
     CFB_TILE_END
 }
 
+// The Chebyshev steps without the z.r sum, one row per thread (as the
+// single-system kernels): block q takes the rows NT (q mod SUB) .. + NT of
+// active tile q / SUB.  The grid covers every tile; blocks past the active
+// ones return at once.  Same arithmetic per row as kb_cheb_step.
+constexpr int kSubTiles = kTileRows / NT;
+
+template <int MAXW>
+__global__ void __launch_bounds__(NT) kb_cheb_step_rows(BArgs B, const float* zin, const float* win,
+                                                        float* wout, float* zout, int j)
+{
+    const int k = blockIdx.x / kSubTiles;
+    if (k >= B.counters[2]) return;
+    const int t = B.actTiles[k];
+    const int s = B.tiles[t].x;
+    if (B.st[s].done) return;
+    const BSys sy = B.sys[s];
+    const int row = B.tiles[t].y + (int)(blockIdx.x % kSubTiles) * NT + (int)threadIdx.x;
+    if (row >= sy.row0 + sy.n) return;
+    const float* cc = B.chebC + (size_t)s * kChebStride;
+    const float c2 = cc[2 * j - 1];
+    const float c3 = cc[2 * j];
+    const float zr = zin[row];
+    const float v = row_f32<MAXW>(B.A, row, __fmul_rn(B.diag32[row], zr),
+                                  [&](int c) { return __ldg(zin + c); });
+    const float r = B.rA[row];
+    const float wn = __fadd_rn(__fmul_rn(c2, win[row]),
+                               __fmul_rn(__fmul_rn(c3, B.rD[row]), __fsub_rn(r, v)));
+    wout[row] = wn;
+    zout[row] = __fadd_rn(zr, wn);
+}
+
 template <int MAXW>
 __global__ void __launch_bounds__(NT) kb_pcg_p_spmv(BArgs B, const float* wA)
 {
@@ -1123,8 +1154,8 @@ int launch_body(cf_batch* bt, int order, cudaGraphConditionalHandle h, int useCo
             }
             else
             {
-                auto fn = kb_cheb_step<false, MW>;
-                fn<<<tgrid(bt, (const void*)fn), NT, 0, s>>>(B, zin, win, B.W1, Z[j & 1], j);
+                kb_cheb_step_rows<MW><<<bt->nTiles * kSubTiles, NT, 0, s>>>(B, zin, win, B.W1,
+                                                                           Z[j & 1], j);
             }
             CFB_LAUNCH();
         }
