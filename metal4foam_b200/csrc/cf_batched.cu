@@ -479,35 +479,37 @@ __global__ void __launch_bounds__(NT) kb_cheb_step(BArgs B, const float* zin, co
     CFB_TILE_END
 }
 
-// The Chebyshev steps without the z.r sum, one row per thread (as the
-// single-system kernels): block q takes the rows NT (q mod SUB) .. + NT of
-// active tile q / SUB.  The grid covers every tile; blocks past the active
-// ones return at once.  Same arithmetic per row as kb_cheb_step.
+// The Chebyshev steps without the z.r sum, one row per thread per pass (as
+// the single-system kernels): sub-tile q (NT rows) is the rows
+// NT (q mod SUB) .. + NT of active tile q / SUB; block b takes the
+// sub-tiles b, b + gridDim.x, ...  Same arithmetic per row as kb_cheb_step.
 constexpr int kSubTiles = kTileRows / NT;
 
 template <int MAXW>
 __global__ void __launch_bounds__(NT) kb_cheb_step_rows(BArgs B, const float* zin, const float* win,
                                                         float* wout, float* zout, int j)
 {
-    const int k = blockIdx.x / kSubTiles;
-    if (k >= B.counters[2]) return;
-    const int t = B.actTiles[k];
-    const int s = B.tiles[t].x;
-    if (B.st[s].done) return;
-    const BSys sy = B.sys[s];
-    const int row = B.tiles[t].y + (int)(blockIdx.x % kSubTiles) * NT + (int)threadIdx.x;
-    if (row >= sy.row0 + sy.n) return;
-    const float* cc = B.chebC + (size_t)s * kChebStride;
-    const float c2 = cc[2 * j - 1];
-    const float c3 = cc[2 * j];
-    const float zr = zin[row];
-    const float v = row_f32<MAXW>(B.A, row, __fmul_rn(B.diag32[row], zr),
-                                  [&](int c) { return __ldg(zin + c); });
-    const float r = B.rA[row];
-    const float wn = __fadd_rn(__fmul_rn(c2, win[row]),
-                               __fmul_rn(__fmul_rn(c3, B.rD[row]), __fsub_rn(r, v)));
-    wout[row] = wn;
-    zout[row] = __fadd_rn(zr, wn);
+    const int nSub = B.counters[2] * kSubTiles;
+    for (int q = blockIdx.x; q < nSub; q += gridDim.x)
+    {
+        const int t = B.actTiles[q / kSubTiles];
+        const int s = B.tiles[t].x;
+        if (B.st[s].done) continue;
+        const BSys sy = B.sys[s];
+        const int row = B.tiles[t].y + (q % kSubTiles) * NT + (int)threadIdx.x;
+        if (row >= sy.row0 + sy.n) continue;
+        const float* cc = B.chebC + (size_t)s * kChebStride;
+        const float c2 = cc[2 * j - 1];
+        const float c3 = cc[2 * j];
+        const float zr = zin[row];
+        const float v = row_f32<MAXW>(B.A, row, __fmul_rn(B.diag32[row], zr),
+                                      [&](int c) { return __ldg(zin + c); });
+        const float r = B.rA[row];
+        const float wn = __fadd_rn(__fmul_rn(c2, win[row]),
+                                   __fmul_rn(__fmul_rn(c3, B.rD[row]), __fsub_rn(r, v)));
+        wout[row] = wn;
+        zout[row] = __fadd_rn(zr, wn);
+    }
 }
 
 template <int MAXW>
@@ -1154,8 +1156,13 @@ int launch_body(cf_batch* bt, int order, cudaGraphConditionalHandle h, int useCo
             }
             else
             {
-                kb_cheb_step_rows<MW><<<bt->nTiles * kSubTiles, NT, 0, s>>>(B, zin, win, B.W1,
-                                                                           Z[j & 1], j);
+                // one pass over up to 4 resident grids of sub-tiles: a batch
+                // of small systems gets one row per thread, a batch whose
+                // tiles would need many more blocks loops instead of
+                // launching blocks that find no active tile
+                const int g = (int)std::min<long long>((long long)bt->nTiles * kSubTiles,
+                                                       4LL * bt->numSMs * bt->maxBlocksPerSM);
+                kb_cheb_step_rows<MW><<<g, NT, 0, s>>>(B, zin, win, B.W1, Z[j & 1], j);
             }
             CFB_LAUNCH();
         }
