@@ -352,7 +352,10 @@ int cf_batch_solve_device(cf_batch* batch, int32_t solver, double* const* psi,
  * (cf_set_spmv_config):
  *   rhsTile 0 (default): the components run at once as single solves, up
  *     to 8 side by side, each on its own stream and host thread, with the
- *     matrix stored once (the context's arrays, read by all);
+ *     matrix stored once (the context's arrays, read by all).  The first
+ *     call allocates the vectors of min(nrhs, 8) solves (116 bytes per
+ *     cell each), kept until the topology changes or the context is
+ *     destroyed;
  *   rhsTile 1..4: fused passes in which every SpMV reads the matrix once
  *     for up to rhsTile components.
  * In both, each component keeps its own scalars, early exit, stopping tests
