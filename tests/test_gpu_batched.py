@@ -126,16 +126,22 @@ def test_c4_batch_48_systems(require_gpu):
     test fires during CG's non-monotone residual phase and 9 outer passes
     do not reach 1e-6), so both paths run with stagnationLimit 400 and
     maxRestarts 20."""
+    import torch
     systems = mesh.batched_systems()
     opts = _lib.default_options(stagnationLimit=400, maxRestarts=20, maxIter=20000)
     bt = make_batch(systems)
     psis = [np.zeros(s.n) for s in systems]
     perfs = bt.solve(psis, [s.source for s in systems], opts)
+    # the default solo size: three 256-row blocks per SM
+    solo_min = torch.cuda.get_device_properties(0).multi_processor_count * 768
+    assert any(s.n >= solo_min for s in systems) and any(s.n < solo_min for s in systems)
     for s, psi, p in zip(systems, psis, perfs):
         assert p.converged and p.finalResidual < 1e-6, s.name
-        _, p1 = single_solve(s, opts)
+        x1, p1 = single_solve(s, opts)
         assert close_iters(p.nIterations, p1.nIterations), (s.name, p.nIterations,
                                                             p1.nIterations)
+        if s.n >= solo_min:          # a solo system: cf_solve's path and result
+            assert np.array_equal(psi, x1) and p.nIterations == p1.nIterations, s.name
         r = s.source - mesh.amul_numpy(s, psi)
         assert np.sum(np.abs(r)) / p.normFactor < 1.01e-6
     bt.close()
