@@ -1,5 +1,6 @@
 """Batched solves (the design's batching row): many independent pressure
-systems of uneven sizes through one launch per phase.  Each system must
+systems of uneven sizes through one launch per phase (the large ones as
+single solves on their own streams beside it).  Each system must
 behave as it does alone: converged to the same FP64 tolerance, the same
 driver decisions (deflation, Gershgorin bound), iteration counts within 10%
 of the single-system path, and the solution within the same distance of an
